@@ -1,0 +1,170 @@
+/*
+ * zolo_b200.h -- C-ABI of the B200 (sm_100a) polar-decomposition / SVD path.
+ *
+ * Drop-in boundary for the reference's Fortran entry points on a 1x1 process
+ * grid.  Each reference-named function keeps the reference's argument list
+ * and meaning; its comment cites the reference interface it replaces
+ * (file:line in shengguolsg/Zolo-SVD).  All matrices are column-major FP64
+ * (DOUBLE PRECISION), integers are 32-bit (MKL LP64 INTEGER), CHARACTER
+ * arguments are passed as `char` in the C names and as `const char*` plus a
+ * trailing hidden `size_t` length in the gfortran-mangled names.
+ *
+ * Descriptors (DESC(9) = DTYPE_, CTXT_, M_, N_, MB_, NB_, RSRC_, CSRC_, LLD_)
+ * must describe a 1x1 grid: DTYPE_ = 1, RSRC_ = CSRC_ = 0, LLD_ >= max(1,M_);
+ * CTXT_ is ignored and IA = JA = IQ = JQ = 1.
+ *
+ * INFO conventions follow the reference: 0 success, -i for a bad scalar
+ * argument i, -(i*100+j) for entry j of array argument i, -12 / -16 for a
+ * too-small LWORK / LWORK2 (pqdwhfacs.f90:286-294), > 0 from a factorisation.
+ * GPU failures are reported as INFO = -1000 - cudaError_t.  Nothing aborts.
+ *
+ * Threading: every handle owns one CUDA stream; calls on one handle are
+ * serialised by a mutex.  The reference-named host-array entry points use a
+ * process-wide default handle on device 0 (or ZOLO_DEVICE).
+ */
+#ifndef ZOLO_B200_H
+#define ZOLO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct zolo_handle_s* zolo_handle_t;
+
+typedef struct {
+  int iterations;      /* polar iterations executed                       */
+  int qr_iterations;   /* of which used the QR form                       */
+  int chol_iterations; /* of which used the Cholesky form                 */
+  int info;            /* first factorisation INFO seen (0 = none)        */
+  double alpha;        /* upper bound used (||A - sigma I||_F)            */
+  double beta;         /* lower bound used                                */
+  double last_err;     /* last ||X_{k+1} - X_k||_F                        */
+  double ms_total;     /* device time of the whole call (CUDA events)     */
+  double ms_bounds;
+  double ms_iter;
+  double ms_h;
+  double flops;        /* canonical FP64 flops of the executed steps      */
+  int64_t launches;    /* kernels launched                                */
+  double con[16];      /* per iteration: CON (Zolo) or c_k (QDWH)         */
+  double err[16];      /* per iteration: ||X_{k+1} - X_k||_F              */
+  int branch[16];      /* per iteration: 1 = QR form, 2 = Cholesky form   */
+} zolo_stats_t;
+
+/* ---- handles (no reference counterpart: the reference is one MPI job) ---- */
+int zolo_create(int device, zolo_handle_t* handle);
+int zolo_destroy(zolo_handle_t handle);
+int zolo_set_stream(zolo_handle_t handle, void* cuda_stream);
+int zolo_get_stats(zolo_handle_t handle, zolo_stats_t* out);
+int zolo_default_handle(zolo_handle_t* handle);
+int zolo_release_workspace(zolo_handle_t handle);
+const char* zolo_version(void);
+
+/* ---- host scalar routines (no GPU needed) ---- */
+/* Compute_Coeff (Auxil_Zolo.f90:165-200): coeff[0:2rk] = c_i, coeff[2rk:3rk] = -a_i. */
+int zolo_compute_coeff(double con, double tol, int rk, double* coeff);
+/* mellipke (Auxil_Zolo.f90:36-71) */
+void zolo_mellipke(double alpha, double tol, double* k, double* e);
+/* MELLIPJ (Auxil_Zolo.f90:73-128) */
+void zolo_mellipj(double u, double alpha, double tol, double* sn, double* cn, double* dn);
+/* choosem (Auxil_Zolo.f90:130-163) */
+int zolo_choosem(double con);
+/* hfunc (hfunc.f90:204-244) */
+double zolo_hfunc(double x);
+/* FONE and next CON of a Zolo iteration (pzolopd1.f90:459-472) */
+void zolo_fone_next(double con, const double* coeff, int rk, double* fone, double* next_con);
+
+/* ---- reference-named entry points, host arrays ---- */
+/* PQDWHFACS (pqdwhfacs.f90:2-3): QDWH-PD of A - SIGMA*I; Q = polar factor,
+ * WORK2 = H = sym(Q^T A) when POLAR = 'T'.  LWORK = -1 or LWORK2 = -1 is a
+ * workspace query (WORK(1), WORK(2)).  TAU is not referenced. */
+void zolo_pqdwhfacs(char sym, int m, int n, double sigma, const double* a, int ia, int ja, const int* desca,
+                    double* q, int iq, int jq, const int* descq, double* work, int lwork, const int* descw,
+                    double* tau, double* work2, int lwork2, int* info, char polar);
+/* ZOLOPD (zolopd.f90:2-3): older QDWH entry (no SYM, BETA = rcond/sqrt(n), W^{-1} X solve, no IT cap). */
+void zolo_zolopd(int m, int n, double sigma, const double* a, int ia, int ja, const int* desca, double* q, int iq,
+                 int jq, const int* descq, double* work, int lwork, const int* descw, double* tau, double* work2,
+                 int lwork2, int* info, char polar);
+/* PZOLOPD1 (pzolopd1.f90:2): Zolo-PD with RK terms from the bounds ALPHA, BETA; Q = polar factor. */
+void zolo_pzolopd1(char sym, int rk, int m, int n, double alpha, double beta, const double* as, int ia, int ja,
+                   const int* desca, double* q, int iq, int jq, const int* descq, int* info, char polar);
+/* PZOLOPD2 (pzolopd2.f90:2): same contract as PZOLOPD1 (the reference's restart variant does not link). */
+void zolo_pzolopd2(char sym, int rk, int m, int n, double alpha, double beta, const double* as, int ia, int ja,
+                   const int* desca, double* q, int iq, int jq, const int* descq, int* info, char polar);
+
+/* gfortran-mangled aliases: all arguments by reference, hidden CHARACTER lengths last */
+void pqdwhfacs_(const char* sym, const int* m, const int* n, const double* sigma, const double* a, const int* ia,
+                const int* ja, const int* desca, double* q, const int* iq, const int* jq, const int* descq,
+                double* work, const int* lwork, const int* descw, double* tau, double* work2, const int* lwork2,
+                int* info, const char* polar, size_t sym_len, size_t polar_len);
+void zolopd_(const int* m, const int* n, const double* sigma, const double* a, const int* ia, const int* ja,
+             const int* desca, double* q, const int* iq, const int* jq, const int* descq, double* work,
+             const int* lwork, const int* descw, double* tau, double* work2, const int* lwork2, int* info,
+             const char* polar, size_t polar_len);
+void pzolopd1_(const char* sym, const int* rk, const int* m, const int* n, const double* alpha, const double* beta,
+               const double* as, const int* ia, const int* ja, const int* desca, double* q, const int* iq,
+               const int* jq, const int* descq, int* info, const char* polar, size_t sym_len, size_t polar_len);
+void pzolopd2_(const char* sym, const int* rk, const int* m, const int* n, const double* alpha, const double* beta,
+               const double* as, const int* ia, const int* ja, const int* desca, double* q, const int* iq,
+               const int* jq, const int* descq, int* info, const char* polar, size_t sym_len, size_t polar_len);
+
+/* ---- device-pointer entry points (the hot path; no host copies) ---- */
+/* QDWH-PD of A - sigma I on device arrays (m >= n).  bounds_mode 0 = PQDWHFACS form,
+ * 1 = ZOLOPD form; left_solve != 0 reproduces ZOLOPD's W^{-1} X solve; maxit < 0: no cap.
+ * dH may be NULL.  Returns INFO. */
+int zolo_qdwh_dev(zolo_handle_t h, char sym, int m, int n, double sigma, const double* dA, int64_t lda, double* dQ,
+                  int64_t ldq, double* dH, int64_t ldh, int bounds_mode, int maxit, int left_solve);
+/* Zolo-PD (PZOLOPD1 semantics) on device arrays; dH may be NULL.  Returns INFO. */
+int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
+                      int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh);
+/* The driver's bounds (test_zolodrv1.f90:167-189 replaced by a QR + R^{-1} estimate):
+ * alpha = ||A||_F, beta = 1/(sqrt(n) ||R^{-1}||_1) for A/alpha = QR (mode 1) or
+ * ||A/alpha||_1 / (sqrt(n) ||R^{-1}||_1) (mode 0). */
+int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* dA, int64_t lda, int mode,
+                    double* alpha, double* beta);
+/* H = (Q^T A + A^T Q)/2 (pqdwhfacs.f90:460-466, ZoloCHK1.f90:80-83). */
+int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda,
+                    double* dH, int64_t ldh);
+
+/* ---- kernel-level entry points (building blocks, used by the parity tests) ---- */
+/* C = alpha op(A) op(B) + beta C (PDGEMM on a 1x1 grid); tri = lower-triangle-only output,
+ * kfrom_n = op(B) is lower triangular (TRMM-like skip). */
+int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
+                   int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
+                   int kfrom_n);
+/* Lower Cholesky in place (PDPOTRF 'L'); returns LAPACK INFO. */
+int zolo_dpotrf_dev(zolo_handle_t h, int n, double* dA, int64_t lda);
+/* Y = X L^{-T} (trans = 'T') or Y = X L^{-1} (trans = 'N'); X is overwritten (workspace). */
+int zolo_dtrsm_dev(zolo_handle_t h, char trans, int m, int n, const double* dL, int64_t ldl, double* dX, int64_t ldx,
+                   double* dY, int64_t ldy);
+/* Structured Householder QR (MPDGEQRF, mpdgeqrf.f:5-324): mtot x n in place; m_top < 0 = unstructured.
+ * dT receives ceil(n/32) blocks of 32x32 compact-WY factors. */
+int zolo_dgeqrf_dev(zolo_handle_t h, int mtot, int n, int m_top, double* dW, int64_t ldw, double* dtau, double* dT);
+/* Explicit Q (MPDORGQR, mpdorgqr.f:5-348) from zolo_dgeqrf_dev's output. */
+int zolo_dorgqr_dev(zolo_handle_t h, int mtot, int n, int m_top, const double* dW, int64_t ldw, const double* dT,
+                    double* dQ, int64_t ldq);
+/* One Zolotarev term through ZOLOQR (zoloqr.f90:82-112): Z = (a/sqrt(c)) Q1 Q2^T of [X; sqrt(c) I]. */
+int zolo_zoloqr_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t ldx, double c, double a, double* dZ,
+                    int64_t ldz);
+/* One Zolotarev term through ZOLOCHOL (zolochol.f90:87-113): Z = a X (X^T X + c I)^{-1}. */
+int zolo_zolochol_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t ldx, double c, double a, double* dZ,
+                      int64_t ldz);
+/* FormX2 (FormX2.f90:73-89): X <- (X + Z)/fone; returns ||X_new - X_old||_F in *err. */
+int zolo_formx2_dev(zolo_handle_t h, int m, int n, double fone, double* dX, int64_t ldx, const double* dZ,
+                    int64_t ldz, double* err);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZOLO_B200_H */

@@ -1,0 +1,320 @@
+"""zolo-svd_b200: B200-native QDWH-PD / Zolo-PD / Zolo-SVD.
+
+Python mirror of the reference's entry points (shengguolsg/Zolo-SVD) over the
+C-ABI of ``include/zolo_b200.h``:
+
+* ``pqdwhfacs``  -- PQDWHFACS (pqdwhfacs.f90:2-3)
+* ``zolopd``     -- ZOLOPD    (zolopd.f90:2-3)
+* ``pzolopd1``   -- PZOLOPD1  (pzolopd1.f90:2)
+* ``compute_coeff``, ``hfunc``, ``choosem`` -- Auxil_Zolo.f90 / hfunc.f90
+
+The host-array functions take NumPy arrays (any layout; they are passed as
+Fortran-ordered copies) and return INFO with the reference's conventions.  The
+``*_dev`` functions take device pointers / CUDA tensors in column-major form
+(see ``colmajor_to_device``).  Every computation runs in the CUDA library; if
+the library is missing this module raises instead of falling back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzolo_b200.so")
+_lib = None
+
+c_double_p = C.POINTER(C.c_double)
+c_int_p = C.POINTER(C.c_int)
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("qr_iterations", C.c_int),
+        ("chol_iterations", C.c_int),
+        ("info", C.c_int),
+        ("alpha", C.c_double),
+        ("beta", C.c_double),
+        ("last_err", C.c_double),
+        ("ms_total", C.c_double),
+        ("ms_bounds", C.c_double),
+        ("ms_iter", C.c_double),
+        ("ms_h", C.c_double),
+        ("flops", C.c_double),
+        ("launches", C.c_int64),
+        ("con", C.c_double * 16),
+        ("err", C.c_double * 16),
+        ("branch", C.c_int * 16),
+    ]
+
+    def as_dict(self) -> dict:
+        it = self.iterations
+        return dict(iterations=it, qr_iterations=self.qr_iterations, chol_iterations=self.chol_iterations,
+                    info=self.info, alpha=self.alpha, beta=self.beta, last_err=self.last_err,
+                    ms_total=self.ms_total, ms_bounds=self.ms_bounds, ms_iter=self.ms_iter, ms_h=self.ms_h,
+                    flops=self.flops, launches=int(self.launches),
+                    con=list(self.con[: min(it, 16)]), err=list(self.err[: min(it, 16)]),
+                    branches=["QR" if b == 1 else "CH" for b in self.branch[: min(it, 16)]])
+
+
+# (name, restype, argtypes)
+_SIGS = [
+    ("zolo_version", C.c_char_p, []),
+    ("zolo_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("zolo_destroy", C.c_int, [C.c_void_p]),
+    ("zolo_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("zolo_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    ("zolo_default_handle", C.c_int, [C.POINTER(C.c_void_p)]),
+    ("zolo_release_workspace", C.c_int, [C.c_void_p]),
+    ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
+    ("zolo_mellipke", None, [C.c_double, C.c_double, c_double_p, c_double_p]),
+    ("zolo_mellipj", None, [C.c_double, C.c_double, C.c_double, c_double_p, c_double_p, c_double_p]),
+    ("zolo_choosem", C.c_int, [C.c_double]),
+    ("zolo_hfunc", C.c_double, [C.c_double]),
+    ("zolo_fone_next", None, [C.c_double, c_double_p, C.c_int, c_double_p, c_double_p]),
+    ("zolo_pqdwhfacs", None, [C.c_char, C.c_int, C.c_int, C.c_double, c_double_p, C.c_int, C.c_int, c_int_p,
+                              c_double_p, C.c_int, C.c_int, c_int_p, c_double_p, C.c_int, c_int_p, c_double_p,
+                              c_double_p, C.c_int, c_int_p, C.c_char]),
+    ("zolo_zolopd", None, [C.c_int, C.c_int, C.c_double, c_double_p, C.c_int, C.c_int, c_int_p, c_double_p,
+                           C.c_int, C.c_int, c_int_p, c_double_p, C.c_int, c_int_p, c_double_p, c_double_p,
+                           C.c_int, c_int_p, C.c_char]),
+    ("zolo_pzolopd1", None, [C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, c_double_p, C.c_int,
+                             C.c_int, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p, C.c_char]),
+    ("zolo_pzolopd2", None, [C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, c_double_p, C.c_int,
+                             C.c_int, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p, C.c_char]),
+    ("zolo_qdwh_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64,
+                                C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int]),
+    ("zolo_pzolopd1_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                    C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64]),
+    ("zolo_bounds_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64, C.c_int,
+                                  c_double_p, c_double_p]),
+    ("zolo_form_h_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                  C.c_void_p, C.c_int64]),
+    ("zolo_dgemm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double,
+                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_int64,
+                                 C.c_int, C.c_int]),
+    ("zolo_dpotrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
+    ("zolo_dtrsm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                                 C.c_int64, C.c_void_p, C.c_int64]),
+    ("zolo_dgeqrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                                  C.c_void_p]),
+    ("zolo_dorgqr_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                                  C.c_void_p, C.c_int64]),
+    ("zolo_zoloqr_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_double, C.c_double,
+                                  C.c_void_p, C.c_int64]),
+    ("zolo_zolochol_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_double, C.c_double,
+                                    C.c_void_p, C.c_int64]),
+    ("zolo_formx2_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64, C.c_void_p,
+                                  C.c_int64, c_double_p]),
+]
+
+EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_"]
+
+
+class ZoloError(RuntimeError):
+    """A negative INFO from the library (argument error or GPU failure)."""
+
+    def __init__(self, where: str, info: int):
+        self.info = info
+        if info <= -1000:
+            msg = f"{where}: CUDA error {-1000 - info}"
+        else:
+            msg = f"{where}: INFO = {info}"
+        super().__init__(msg)
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library (built in-tree); raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python zolo-svd_b200/build.py` "
+                               "(this package has no CPU fallback)")
+        l = C.CDLL(LIB_PATH)
+        for name, res, args in _SIGS:
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(c_double_p)
+
+
+def _desc(m: int, n: int, nb: int = 64, lld: int | None = None) -> np.ndarray:
+    return np.array([1, 0, m, n, nb, nb, 0, 0, max(1, m if lld is None else lld)], dtype=np.int32)
+
+
+# ---------------------------------------------------------------------------
+# host scalar routines
+# ---------------------------------------------------------------------------
+def compute_coeff(con: float, tol: float, rk: int) -> np.ndarray:
+    out = np.zeros(3 * rk)
+    r = lib().zolo_compute_coeff(con, tol, rk, _dp(out))
+    if r != 0:
+        raise ZoloError("zolo_compute_coeff", r)
+    return out
+
+
+def hfunc(x: float) -> float:
+    return float(lib().zolo_hfunc(x))
+
+
+def choosem(con: float) -> int:
+    return int(lib().zolo_choosem(con))
+
+
+def fone_next(con: float, coeff: np.ndarray, rk: int) -> tuple[float, float]:
+    f, nx = C.c_double(), C.c_double()
+    c = np.ascontiguousarray(coeff, dtype=np.float64)
+    lib().zolo_fone_next(con, _dp(c), rk, C.byref(f), C.byref(nx))
+    return f.value, nx.value
+
+
+# ---------------------------------------------------------------------------
+# reference-named host-array entry points
+# ---------------------------------------------------------------------------
+def workspace_query(m: int, n: int, nb: int = 64) -> tuple[int, int]:
+    """LWORK = -1 query of PQDWHFACS: the minimal LWORK and LWORK2."""
+    work = np.zeros(2)
+    info = C.c_int(0)
+    d = _desc(m, n, nb)
+    dw = _desc(2 * n, n, nb)
+    dummy = np.zeros(1)
+    lib().zolo_pqdwhfacs(b"N", m, n, 0.0, _dp(dummy), 1, 1, d.ctypes.data_as(c_int_p), _dp(dummy), 1, 1,
+                         d.ctypes.data_as(c_int_p), _dp(work), -1, dw.ctypes.data_as(c_int_p), _dp(dummy),
+                         _dp(dummy), -1, C.byref(info), b"N")
+    return int(work[0]), int(work[1])
+
+
+def pqdwhfacs(sym: str, a: np.ndarray, sigma: float = 0.0, polar: str = "T", nb: int = 64):
+    """PQDWHFACS on a host matrix: returns (Q, H or None, INFO)."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    m, n = a.shape
+    lw, lw2 = workspace_query(m, n, nb)
+    q = np.zeros((m, n), order="F")
+    work = np.zeros(max(lw, 2))
+    work2 = np.zeros((max(lw2, n * n),))
+    tau = np.zeros(max(n, 1))
+    d = _desc(m, n, nb)
+    dw = _desc(2 * n, n, nb)
+    info = C.c_int(0)
+    lib().zolo_pqdwhfacs(sym.encode()[:1], m, n, sigma, _dp(a), 1, 1, d.ctypes.data_as(c_int_p), _dp(q), 1, 1,
+                         d.ctypes.data_as(c_int_p), _dp(work), len(work), dw.ctypes.data_as(c_int_p), _dp(tau),
+                         _dp(work2), len(work2), C.byref(info), polar.encode()[:1])
+    h = None
+    if polar.upper().startswith("T") and info.value == 0:
+        h = np.asfortranarray(work2[: m * n].reshape((m, n), order="F")[:n, :])
+    return q, h, info.value
+
+
+def zolopd(a: np.ndarray, sigma: float = 0.0, polar: str = "T", nb: int = 64):
+    """ZOLOPD on a host matrix: returns (Q, H or None, INFO)."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    m, n = a.shape
+    lw, lw2 = workspace_query(m, n, nb)
+    q = np.zeros((m, n), order="F")
+    work = np.zeros(max(lw, 2))
+    work2 = np.zeros((max(lw2, n * n),))
+    tau = np.zeros(max(n, 1))
+    d = _desc(m, n, nb)
+    dw = _desc(2 * n, n, nb)
+    info = C.c_int(0)
+    lib().zolo_zolopd(m, n, sigma, _dp(a), 1, 1, d.ctypes.data_as(c_int_p), _dp(q), 1, 1,
+                      d.ctypes.data_as(c_int_p), _dp(work), len(work), dw.ctypes.data_as(c_int_p), _dp(tau),
+                      _dp(work2), len(work2), C.byref(info), polar.encode()[:1])
+    h = None
+    if polar.upper().startswith("T") and info.value == 0:
+        h = np.asfortranarray(work2[: m * n].reshape((m, n), order="F")[:n, :])
+    return q, h, info.value
+
+
+def pzolopd1(sym: str, rk: int, a: np.ndarray, alpha: float, beta: float, polar: str = "N", nb: int = 64):
+    """PZOLOPD1 on a host matrix: returns (Q, INFO)."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    m, n = a.shape
+    q = np.zeros((m, n), order="F")
+    d = _desc(m, n, nb)
+    info = C.c_int(0)
+    lib().zolo_pzolopd1(sym.encode()[:1], rk, m, n, alpha, beta, _dp(a), 1, 1, d.ctypes.data_as(c_int_p), _dp(q),
+                        1, 1, d.ctypes.data_as(c_int_p), C.byref(info), polar.encode()[:1])
+    return q, info.value
+
+
+# ---------------------------------------------------------------------------
+# device-pointer API
+# ---------------------------------------------------------------------------
+class Handle:
+    """A library handle (one CUDA stream, cached workspace)."""
+
+    def __init__(self, device: int = 0):
+        self.ptr = C.c_void_p()
+        r = lib().zolo_create(device, C.byref(self.ptr))
+        if r != 0:
+            raise ZoloError("zolo_create", r)
+
+    def close(self):
+        if self.ptr:
+            lib().zolo_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        r = lib().zolo_set_stream(self.ptr, C.c_void_p(stream_ptr))
+        if r != 0:
+            raise ZoloError("zolo_set_stream", r)
+
+    def stats(self) -> dict:
+        s = Stats()
+        lib().zolo_get_stats(self.ptr, C.byref(s))
+        return s.as_dict()
+
+    def release(self):
+        lib().zolo_release_workspace(self.ptr)
+
+
+def colmajor_to_device(a: np.ndarray, device="cuda"):
+    """Copy an m x n host matrix to a CUDA tensor holding it column-major (ld = m).
+
+    The tensor has shape (n, m): tensor[j, i] == a[i, j].
+    """
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float64).T)).to(device)
+
+
+def device_to_colmajor(t) -> np.ndarray:
+    """Inverse of ``colmajor_to_device``."""
+    return np.asfortranarray(t.detach().cpu().numpy().T)
+
+
+def _ck(name: str, r: int) -> int:
+    if r < 0:
+        raise ZoloError(name, r)
+    return r
+
+
+def qdwh_dev(h: Handle, sym: str, m: int, n: int, sigma: float, dA: int, lda: int, dQ: int, ldq: int,
+             dH: int = 0, ldh: int = 1, bounds_mode: int = 0, maxit: int = 12, left_solve: int = 0) -> int:
+    return _ck("zolo_qdwh_dev", lib().zolo_qdwh_dev(h.ptr, sym.encode()[:1], m, n, sigma, dA, lda, dQ, ldq,
+                                                   dH or None, ldh, bounds_mode, maxit, left_solve))
+
+
+def pzolopd1_dev(h: Handle, sym: str, rk: int, m: int, n: int, alpha: float, beta: float, dA: int, lda: int,
+                 dQ: int, ldq: int, dH: int = 0, ldh: int = 1) -> int:
+    return _ck("zolo_pzolopd1_dev", lib().zolo_pzolopd1_dev(h.ptr, sym.encode()[:1], rk, m, n, alpha, beta, dA, lda,
+                                                           dQ, ldq, dH or None, ldh))
+
+
+def bounds_dev(h: Handle, m: int, n: int, dA: int, lda: int, mode: int = 1, sigma: float = 0.0):
+    al, be = C.c_double(), C.c_double()
+    r = lib().zolo_bounds_dev(h.ptr, m, n, sigma, dA, lda, mode, C.byref(al), C.byref(be))
+    return al.value, be.value, _ck("zolo_bounds_dev", r)

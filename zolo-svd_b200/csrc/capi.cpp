@@ -1,0 +1,459 @@
+// extern "C" boundary: handles, reference-named host-array entry points
+// (1x1-grid descriptors, workspace queries, INFO codes) and the device-pointer
+// hot path.  See include/zolo_b200.h for the contract of every symbol.
+#include "../../include/zolo_b200.h"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "coeff.h"
+#include "context.h"
+#include "linalg.h"
+#include "polar.h"
+
+struct zolo_handle_s {
+  explicit zolo_handle_s(int dev) : ctx(dev) {}
+  zolo::Context ctx;
+};
+
+namespace {
+
+using zolo::Context;
+using zolo::CudaFailure;
+
+constexpr int kCudaBase = -1000;
+
+template <class F>
+int guarded(zolo_handle_t h, F&& f) {
+  if (!h) return -999;
+  std::lock_guard<std::mutex> lk(h->ctx.mu);
+  try {
+    zolo::ck(cudaSetDevice(h->ctx.device()));
+    return f(h->ctx);
+  } catch (const CudaFailure& e) {
+    return kCudaBase - static_cast<int>(e.err);
+  } catch (const std::bad_alloc&) {
+    return kCudaBase - static_cast<int>(cudaErrorMemoryAllocation);
+  }
+}
+
+std::mutex g_default_mu;
+zolo_handle_t g_default = nullptr;
+
+// 1x1-grid descriptor check; returns 0 or the reference-style INFO for argument `pos`.
+int check_desc(const int* desc, int m, int n, int pos) {
+  if (!desc) return -(pos * 100 + 1);
+  if (desc[0] != 1) return -(pos * 100 + 1);
+  if (desc[2] < m) return -(pos * 100 + 3);
+  if (desc[3] < n) return -(pos * 100 + 4);
+  if (desc[6] != 0) return -(pos * 100 + 7);
+  if (desc[7] != 0) return -(pos * 100 + 8);
+  if (desc[8] < std::max(1, desc[2])) return -(pos * 100 + 9);
+  return 0;
+}
+
+// reference workspace minimums on a 1x1 grid (pqdwhfacs.f90:262-278)
+void qdwh_lwork(int m, int n, const int* desca, const int* descw, double* lwin, double* lwin2) {
+  const int nba = desca ? std::max(desca[5], 1) : 64;
+  const int nbw = descw ? std::max(descw[5], 1) : nba;
+  const double gecon = 5.0 * n + nba;                                   // PDGECON LWORK
+  const double geqrf = static_cast<double>(nbw) * (3.0 * n + nbw);      // PDGEQRF LWORK for 2N x N
+  *lwin = std::max(std::max(gecon + 1.0, 2.0 * n * static_cast<double>(n)), 2.0 * m * static_cast<double>(n));
+  *lwin2 = std::max(geqrf + 1.0, static_cast<double>(m) * n);
+}
+
+struct DevBuf {
+  double* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+int run_qdwh_host(char sym, int m, int n, double sigma, const double* a, int ia, int ja, const int* desca, double* q,
+                  int iq, int jq, const int* descq, double* work, int lwork, const int* descw, double* work2,
+                  int lwork2, char polar, bool zolopd_mode) {
+  if (m < n) return -1;
+  const bool query = (lwork == -1 || lwork2 == -1);
+  // argument positions differ between PQDWHFACS and ZOLOPD (no SYM)
+  const int off = zolopd_mode ? -1 : 0;
+  if (m == 0 || n == 0) return 0;
+  double lwin, lwin2;
+  qdwh_lwork(m, n, desca, descw, &lwin, &lwin2);
+  if (work) {  // WORK(1), WORK(2) are always set, as pqdwhfacs.f90:279-280 does
+    work[0] = lwin;
+    work[1] = lwin2;
+  }
+  if (query) return 0;
+  if (ia != 1) return -(6 + off);
+  if (ja != 1) return -(7 + off);
+  if (int e = check_desc(desca, m, n, 8 + off)) return e;
+  if (iq != 1) return -(10 + off);
+  if (jq != 1) return -(11 + off);
+  if (int e = check_desc(descq, m, n, 12 + off)) return e;
+  if (lwork < lwin) return -12;
+  if (lwork2 < lwin2) return -16;
+  zolo_handle_t h = nullptr;
+  if (int e = zolo_default_handle(&h)) return e;
+  const bool want_h = (polar == 'T' || polar == 't');
+  return guarded(h, [&](Context& c) -> int {
+    DevBuf dA, dQ, dH;
+    const int64_t ld = m;
+    zolo::ck(cudaMalloc(&dA.p, sizeof(double) * m * n));
+    zolo::ck(cudaMalloc(&dQ.p, sizeof(double) * m * n));
+    if (want_h) zolo::ck(cudaMalloc(&dH.p, sizeof(double) * n * n));
+    zolo::ck(cudaMemcpy2DAsync(dA.p, ld * sizeof(double), a, desca[8] * sizeof(double), m * sizeof(double), n,
+                               cudaMemcpyHostToDevice, c.stream()));
+    zolo::QdwhOpts o;
+    o.sym = zolopd_mode ? 'N' : sym;
+    o.sigma = sigma;
+    o.bounds = zolopd_mode ? zolo::BOUNDS_ZOLOPD : zolo::BOUNDS_PQDWHFACS;
+    o.maxit = zolopd_mode ? -1 : 12;
+    o.left_solve = zolopd_mode;
+    const int info = zolo::qdwh(c, m, n, dA.p, ld, dQ.p, ld, want_h ? dH.p : nullptr, n, o);
+    zolo::ck(cudaMemcpy2DAsync(q, descq[8] * sizeof(double), dQ.p, ld * sizeof(double), m * sizeof(double), n,
+                               cudaMemcpyDeviceToHost, c.stream()));
+    if (want_h && work2)
+      zolo::ck(cudaMemcpy2DAsync(work2, descq[8] * sizeof(double), dH.p, n * sizeof(double), n * sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, c.stream()));
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return info;
+  });
+}
+
+int run_zolo_host(char sym, int rk, int m, int n, double alpha, double beta, const double* as, int ia, int ja,
+                  const int* desca, double* q, int iq, int jq, const int* descq) {
+  if (rk < 1 || rk > 8) return -2;
+  if (m < n) return -3;
+  if (m == 0 || n == 0) return 0;
+  if (!(alpha > 0.0)) return -5;
+  if (!(beta > 0.0)) return -6;
+  if (ia != 1) return -8;
+  if (ja != 1) return -9;
+  if (int e = check_desc(desca, m, n, 10)) return e;
+  if (iq != 1) return -12;
+  if (jq != 1) return -13;
+  if (int e = check_desc(descq, m, n, 14)) return e;
+  zolo_handle_t h = nullptr;
+  if (int e = zolo_default_handle(&h)) return e;
+  return guarded(h, [&](Context& c) -> int {
+    DevBuf dA, dQ;
+    const int64_t ld = m;
+    zolo::ck(cudaMalloc(&dA.p, sizeof(double) * m * n));
+    zolo::ck(cudaMalloc(&dQ.p, sizeof(double) * m * n));
+    zolo::ck(cudaMemcpy2DAsync(dA.p, ld * sizeof(double), as, desca[8] * sizeof(double), m * sizeof(double), n,
+                               cudaMemcpyHostToDevice, c.stream()));
+    const int info = zolo::zolo_pd(c, sym, rk, m, n, alpha, beta, dA.p, ld, dQ.p, ld, nullptr, 0);
+    zolo::ck(cudaMemcpy2DAsync(q, descq[8] * sizeof(double), dQ.p, ld * sizeof(double), m * sizeof(double), n,
+                               cudaMemcpyDeviceToHost, c.stream()));
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return info;
+  });
+}
+
+inline bool upper(char c) { return c == 'T' || c == 't' || c == 'C' || c == 'c'; }
+
+}  // namespace
+
+extern "C" {
+
+const char* zolo_version(void) { return "zolo-b200 0.1 (sm_100a, FP64 DMMA)"; }
+
+int zolo_create(int device, zolo_handle_t* handle) {
+  if (!handle) return -2;
+  try {
+    *handle = new zolo_handle_s(device);
+    return 0;
+  } catch (const CudaFailure& e) {
+    *handle = nullptr;
+    return kCudaBase - static_cast<int>(e.err);
+  }
+}
+
+int zolo_destroy(zolo_handle_t handle) {
+  if (!handle) return 0;
+  {
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (handle == g_default) g_default = nullptr;
+  }
+  delete handle;
+  return 0;
+}
+
+int zolo_default_handle(zolo_handle_t* handle) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default) {
+    int dev = 0;
+    if (const char* s = std::getenv("ZOLO_DEVICE")) dev = std::atoi(s);
+    const int e = zolo_create(dev, &g_default);
+    if (e) return e;
+  }
+  *handle = g_default;
+  return 0;
+}
+
+int zolo_set_stream(zolo_handle_t h, void* s) {
+  return guarded(h, [&](Context& c) {
+    c.set_stream(static_cast<cudaStream_t>(s));
+    return 0;
+  });
+}
+
+int zolo_release_workspace(zolo_handle_t h) {
+  return guarded(h, [&](Context& c) {
+    c.release_all();
+    return 0;
+  });
+}
+
+int zolo_get_stats(zolo_handle_t h, zolo_stats_t* out) {
+  if (!h || !out) return -2;
+  std::lock_guard<std::mutex> lk(h->ctx.mu);
+  const zolo::Stats& s = h->ctx.stats;
+  out->iterations = s.iterations;
+  out->qr_iterations = s.qr_iterations;
+  out->chol_iterations = s.chol_iterations;
+  out->info = s.info;
+  out->alpha = s.alpha;
+  out->beta = s.beta;
+  out->last_err = s.last_err;
+  out->ms_total = s.ms_total;
+  out->ms_bounds = s.ms_bounds;
+  out->ms_iter = s.ms_iter;
+  out->ms_h = s.ms_h;
+  out->flops = s.flops;
+  out->launches = s.launches;
+  for (int i = 0; i < 16; ++i) {
+    out->con[i] = s.con[i];
+    out->err[i] = s.err[i];
+    out->branch[i] = s.branch[i];
+  }
+  return 0;
+}
+
+int zolo_compute_coeff(double con, double tol, int rk, double* coeff) {
+  if (rk < 1 || rk > 8 || !coeff) return -3;
+  if (!(con >= 1.0)) return -1;
+  zolo::compute_coeff(con, tol, rk, coeff);
+  return 0;
+}
+void zolo_mellipke(double alpha, double tol, double* k, double* e) { zolo::mellipke(alpha, tol, k, e); }
+void zolo_mellipj(double u, double alpha, double tol, double* sn, double* cn, double* dn) {
+  zolo::mellipj(u, alpha, tol, sn, cn, dn);
+}
+int zolo_choosem(double con) { return zolo::choosem(con); }
+double zolo_hfunc(double x) { return zolo::hfunc(x); }
+void zolo_fone_next(double con, const double* coeff, int rk, double* fone, double* next_con) {
+  const double f = zolo::zolo_fone(coeff, rk);
+  if (fone) *fone = f;
+  if (next_con) *next_con = zolo::zolo_next_con(con, coeff, rk, f);
+}
+
+void zolo_pqdwhfacs(char sym, int m, int n, double sigma, const double* a, int ia, int ja, const int* desca,
+                    double* q, int iq, int jq, const int* descq, double* work, int lwork, const int* descw,
+                    double* /*tau*/, double* work2, int lwork2, int* info, char polar) {
+  const int r = run_qdwh_host(sym, m, n, sigma, a, ia, ja, desca, q, iq, jq, descq, work, lwork, descw, work2,
+                              lwork2, polar, false);
+  if (info) *info = r;
+}
+
+void zolo_zolopd(int m, int n, double sigma, const double* a, int ia, int ja, const int* desca, double* q, int iq,
+                 int jq, const int* descq, double* work, int lwork, const int* descw, double* /*tau*/, double* work2,
+                 int lwork2, int* info, char polar) {
+  const int r = run_qdwh_host('N', m, n, sigma, a, ia, ja, desca, q, iq, jq, descq, work, lwork, descw, work2, lwork2,
+                              polar, true);
+  if (info) *info = r;
+}
+
+void zolo_pzolopd1(char sym, int rk, int m, int n, double alpha, double beta, const double* as, int ia, int ja,
+                   const int* desca, double* q, int iq, int jq, const int* descq, int* info, char /*polar*/) {
+  const int r = run_zolo_host(sym, rk, m, n, alpha, beta, as, ia, ja, desca, q, iq, jq, descq);
+  if (info) *info = r;
+}
+
+void zolo_pzolopd2(char sym, int rk, int m, int n, double alpha, double beta, const double* as, int ia, int ja,
+                   const int* desca, double* q, int iq, int jq, const int* descq, int* info, char polar) {
+  zolo_pzolopd1(sym, rk, m, n, alpha, beta, as, ia, ja, desca, q, iq, jq, descq, info, polar);
+}
+
+void pqdwhfacs_(const char* sym, const int* m, const int* n, const double* sigma, const double* a, const int* ia,
+                const int* ja, const int* desca, double* q, const int* iq, const int* jq, const int* descq,
+                double* work, const int* lwork, const int* descw, double* tau, double* work2, const int* lwork2,
+                int* info, const char* polar, size_t, size_t) {
+  zolo_pqdwhfacs(*sym, *m, *n, *sigma, a, *ia, *ja, desca, q, *iq, *jq, descq, work, *lwork, descw, tau, work2,
+                 *lwork2, info, *polar);
+}
+
+void zolopd_(const int* m, const int* n, const double* sigma, const double* a, const int* ia, const int* ja,
+             const int* desca, double* q, const int* iq, const int* jq, const int* descq, double* work,
+             const int* lwork, const int* descw, double* tau, double* work2, const int* lwork2, int* info,
+             const char* polar, size_t) {
+  zolo_zolopd(*m, *n, *sigma, a, *ia, *ja, desca, q, *iq, *jq, descq, work, *lwork, descw, tau, work2, *lwork2, info,
+              *polar);
+}
+
+void pzolopd1_(const char* sym, const int* rk, const int* m, const int* n, const double* alpha, const double* beta,
+               const double* as, const int* ia, const int* ja, const int* desca, double* q, const int* iq,
+               const int* jq, const int* descq, int* info, const char* polar, size_t, size_t) {
+  zolo_pzolopd1(*sym, *rk, *m, *n, *alpha, *beta, as, *ia, *ja, desca, q, *iq, *jq, descq, info, *polar);
+}
+
+void pzolopd2_(const char* sym, const int* rk, const int* m, const int* n, const double* alpha, const double* beta,
+               const double* as, const int* ia, const int* ja, const int* desca, double* q, const int* iq,
+               const int* jq, const int* descq, int* info, const char* polar, size_t, size_t) {
+  zolo_pzolopd2(*sym, *rk, *m, *n, *alpha, *beta, as, *ia, *ja, desca, q, *iq, *jq, descq, info, *polar);
+}
+
+int zolo_qdwh_dev(zolo_handle_t h, char sym, int m, int n, double sigma, const double* dA, int64_t lda, double* dQ,
+                  int64_t ldq, double* dH, int64_t ldh, int bounds_mode, int maxit, int left_solve) {
+  return guarded(h, [&](Context& c) {
+    zolo::QdwhOpts o;
+    o.sym = sym;
+    o.sigma = sigma;
+    o.bounds = bounds_mode ? zolo::BOUNDS_ZOLOPD : zolo::BOUNDS_PQDWHFACS;
+    o.maxit = maxit;
+    o.left_solve = left_solve != 0;
+    return zolo::qdwh(c, m, n, dA, lda, dQ, ldq, dH, ldh, o);
+  });
+}
+
+int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
+                      int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh) {
+  return guarded(h, [&](Context& c) {
+    return zolo::zolo_pd(c, sym, rk, m, n, alpha, beta, dA, lda, dQ, ldq, dH, ldh);
+  });
+}
+
+int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* dA, int64_t lda, int mode,
+                    double* alpha, double* beta) {
+  if (m < n) return -2;
+  return guarded(h, [&](Context& c) {
+    c.stats = zolo::Stats{};
+    return zolo::bounds(c, m, n, sigma, dA, lda, mode ? zolo::BOUNDS_ZOLOPD : zolo::BOUNDS_PQDWHFACS, alpha, beta);
+  });
+}
+
+int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda,
+                    double* dH, int64_t ldh) {
+  return guarded(h, [&](Context& c) {
+    zolo::form_h(c, m, n, dQ, ldq, dA, lda, dH, ldh);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
+                   int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
+                   int kfrom_n) {
+  return guarded(h, [&](Context& c) {
+    zolo::gemm(c, upper(transa), upper(transb), m, n, k, alpha, zolo::Mat{const_cast<double*>(dA), lda, 0},
+               zolo::Mat{const_cast<double*>(dB), ldb, 0}, beta, zolo::Mat{dC, ldc, 0}, 1, nullptr, tri, kfrom_n);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_dpotrf_dev(zolo_handle_t h, int n, double* dA, int64_t lda) {
+  return guarded(h, [&](Context& c) {
+    int* dinfo = c.dinfo();
+    zolo::ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
+    zolo::potrf(c, n, zolo::Mat{dA, lda, 0}, 1, dinfo);
+    int info = 0;
+    zolo::ck(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c.stream()));
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return info;
+  });
+}
+
+int zolo_dtrsm_dev(zolo_handle_t h, char trans, int m, int n, const double* dL, int64_t ldl, double* dX, int64_t ldx,
+                   double* dY, int64_t ldy) {
+  return guarded(h, [&](Context& c) {
+    zolo::Mat L{const_cast<double*>(dL), ldl, 0}, X{dX, ldx, 0}, Y{dY, ldy, 0};
+    if (upper(trans)) zolo::trsm_rlt(c, m, n, L, X, Y, 1);
+    else zolo::trsm_rln(c, m, n, L, X, Y, 1);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_dgeqrf_dev(zolo_handle_t h, int mtot, int n, int m_top, double* dW, int64_t ldw, double* dtau, double* dT) {
+  if (mtot < n) return -2;
+  return guarded(h, [&](Context& c) {
+    zolo::geqrf(c, mtot, n, m_top, zolo::Mat{dW, ldw, 0}, dtau, dT, 1);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_dorgqr_dev(zolo_handle_t h, int mtot, int n, int m_top, const double* dW, int64_t ldw, const double* dT,
+                    double* dQ, int64_t ldq) {
+  if (mtot < n) return -2;
+  return guarded(h, [&](Context& c) {
+    zolo::orgqr(c, mtot, n, m_top, zolo::Mat{const_cast<double*>(dW), ldw, 0}, dT, zolo::Mat{dQ, ldq, 0}, 1);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_zoloqr_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t ldx, double cc, double a, double* dZ,
+                    int64_t ldz) {
+  if (!(cc > 0.0)) return -6;
+  return guarded(h, [&](Context& c) {
+    const int mp = (m + 1) / 2 * 2;
+    const int64_t ldw = (static_cast<int64_t>(mp) + n + 1) / 2 * 2;
+    zolo::Mat W{c.buf("W", static_cast<size_t>(ldw) * n), ldw, 0};
+    zolo::Mat Qf{c.buf("Qf", static_cast<size_t>(ldw) * n), ldw, 0};
+    double* tau = c.buf("tau", n);
+    double* T = c.buf("qr_t", static_cast<size_t>((n + 31) / 32) * 1024);
+    const double s = std::sqrt(cc);
+    zolo::ck(zolo::form_stack(m, mp, n, dX, ldx, W.p, W.ld, 0, nullptr, s, 1, c.stream()));
+    zolo::geqrf(c, mp + n, n, mp, W, tau, T, 1);
+    zolo::orgqr(c, mp + n, n, mp, W, T, Qf, 1);
+    zolo::gemm(c, 0, 1, m, n, n, a / s, Qf, Qf.at(mp, 0), 0.0, zolo::Mat{dZ, ldz, 0}, 1, nullptr, 0, 1);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_zolochol_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t ldx, double cc, double a, double* dZ,
+                      int64_t ldz) {
+  return guarded(h, [&](Context& c) {
+    const int64_t ldn = (n + 1) / 2 * 2, ldm = (m + 1) / 2 * 2;
+    zolo::Mat G{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
+    zolo::Mat Xc{c.buf("Xc", static_cast<size_t>(ldm) * n), ldm, 0};
+    zolo::Mat Y{c.buf("Y", static_cast<size_t>(ldm) * n), ldm, 0};
+    zolo::gemm(c, 1, 0, n, n, m, 1.0, zolo::Mat{const_cast<double*>(dX), ldx, 0},
+               zolo::Mat{const_cast<double*>(dX), ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+    zolo::ck(zolo::add_diag(n, G.p, G.ld, cc, c.stream()));
+    int* dinfo = c.dinfo();
+    zolo::ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
+    zolo::potrf(c, n, G, 1, dinfo);
+    zolo::ck(zolo::scale_copy(m, n, a, dX, ldx, 0, Xc.p, Xc.ld, 0, 1, 0.0, c.stream()));
+    zolo::trsm_rlt(c, m, n, G, Xc, Y, 1);
+    zolo::trsm_rln(c, m, n, G, Y, zolo::Mat{dZ, ldz, 0}, 1);
+    int info = 0;
+    zolo::ck(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c.stream()));
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return info;
+  });
+}
+
+int zolo_formx2_dev(zolo_handle_t h, int m, int n, double fone, double* dX, int64_t ldx, const double* dZ,
+                    int64_t ldz, double* err) {
+  return guarded(h, [&](Context& c) {
+    double* scal = c.dscal();
+    zolo::ck(zolo::combine_update(m, n, dX, ldx, dZ, ldz, 0, 1, 1.0 / fone, 1.0 / fone, nullptr, c.dpartial(), scal,
+                                  c.stream()));
+    double e2 = 0.0;
+    zolo::ck(cudaMemcpyAsync(&e2, scal, sizeof(double), cudaMemcpyDeviceToHost, c.stream()));
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    if (err) *err = std::sqrt(e2);
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+#include "context.h"
+
+namespace zolo {
+
+Context::Context(int device) : device_(device) {
+  ck(cudaSetDevice(device));
+  ck(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+  stream_ = own_stream_;
+}
+
+Context::~Context() {
+  release_all();
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void Context::release_all() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& kv : bufs_) cudaFree(kv.second.first);
+  bufs_.clear();
+  if (splitk_.ptr) cudaFree(splitk_.ptr);
+  splitk_ = Scratch{};
+}
+
+static void* grow(std::map<std::string, std::pair<void*, size_t>>& bufs, const std::string& name, size_t bytes,
+                  cudaStream_t st) {
+  auto it = bufs.find(name);
+  if (it != bufs.end() && it->second.second >= bytes) return it->second.first;
+  if (it != bufs.end()) {
+    // kernels queued on the stream may still use the old block
+    ck(cudaStreamSynchronize(st));
+    ck(cudaFree(it->second.first));
+    bufs.erase(it);
+  }
+  void* p = nullptr;
+  const size_t b = bytes < 256 ? 256 : bytes;
+  ck(cudaMalloc(&p, b));
+  bufs[name] = {p, b};
+  return p;
+}
+
+double* Context::buf(const std::string& name, size_t elems) {
+  return static_cast<double*>(grow(bufs_, name, elems * sizeof(double), stream_));
+}
+
+int* Context::ibuf(const std::string& name, size_t elems) {
+  return static_cast<int*>(grow(bufs_, name, elems * sizeof(int), stream_));
+}
+
+void Context::ensure_splitk(size_t bytes) {
+  if (splitk_.bytes >= bytes) return;
+  if (splitk_.ptr) {
+    ck(cudaStreamSynchronize(stream_));
+    ck(cudaFree(splitk_.ptr));
+  }
+  splitk_.ptr = nullptr;
+  splitk_.bytes = 0;
+  void* p = nullptr;
+  ck(cudaMalloc(&p, bytes));
+  splitk_.ptr = static_cast<double*>(p);
+  splitk_.bytes = bytes;
+}
+
+double* Context::dscal() { return buf("__scal", 64); }
+double* Context::dpartial() { return buf("__partial", 4096); }
+int* Context::dinfo() { return ibuf("__info", 1024); }
+
+}  // namespace zolo

@@ -1,0 +1,68 @@
+// Per-handle state: device, stream, cached device workspace, statistics.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "kernels.h"
+
+namespace zolo {
+
+struct Stats {
+  int iterations = 0;
+  int qr_iterations = 0;
+  int chol_iterations = 0;
+  int info = 0;
+  double alpha = 0.0, beta = 0.0, last_err = 0.0;
+  double ms_total = 0.0, ms_bounds = 0.0, ms_iter = 0.0, ms_h = 0.0;
+  double flops = 0.0;
+  int64_t launches = 0;
+  double con[16] = {0};
+  double err[16] = {0};
+  int branch[16] = {0};  // 1 = QR, 2 = Cholesky
+};
+
+// Thrown inside the library on a CUDA error; converted to an INFO code at the C-ABI.
+struct CudaFailure {
+  cudaError_t err;
+};
+
+inline void ck(cudaError_t e) {
+  if (e != cudaSuccess) throw CudaFailure{e};
+}
+
+class Context {
+ public:
+  explicit Context(int device);
+  ~Context();
+
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+
+  // Named cached device buffer of at least `elems` doubles (grow-only).
+  double* buf(const std::string& name, size_t elems);
+  int* ibuf(const std::string& name, size_t elems);
+  Scratch& splitk() { return splitk_; }
+  void ensure_splitk(size_t bytes);
+  void release_all();
+
+  Stats stats;
+  std::mutex mu;
+
+  // small device scalars / partial sums
+  double* dscal();     // 64 doubles
+  double* dpartial();  // 4096 doubles
+  int* dinfo();        // 1024 ints
+
+ private:
+  int device_;
+  cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+  std::map<std::string, std::pair<void*, size_t>> bufs_;
+  Scratch splitk_;
+};
+
+}  // namespace zolo

@@ -1,0 +1,385 @@
+// FP64 GEMM on the sm_100a FP64 tensor path (DMMA mma.sync.m16n8k8.f64).
+//
+// tcgen05.mma has no FP64 kind, so the FP64 contractions of the polar
+// iterations (Gram matrix, TRSM updates, Householder trailing updates,
+// Q1*Q2^T) run on DMMA.  CTA tile 128x128x16, 8 warps (2 x 4), warp tile
+// 64x32, 4-stage cp.async pipeline, padded shared-memory layouts chosen so
+// every fragment load is a conflict-free LDS.128 (or LDS.64 for op(B)=B^T).
+//
+// Index permutations (free because they are applied consistently):
+//   * inside each 16-row MMA tile, logical row g <-> physical row 2g and
+//     logical row g+8 <-> physical row 2g+1, so a thread's two A rows are
+//     adjacent in memory;
+//   * inside each 8-wide k step, logical k slot t <-> physical k 2t and slot
+//     t+4 <-> 2t+1 for both operands, so a thread's two k values are adjacent.
+#include "common.cuh"
+#include "kernels.h"
+
+#include <algorithm>
+
+namespace zolo {
+
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, NT = 256;
+constexpr int LDA_N = BM + 2;  // sA[k][m]  (op(A) = A)
+constexpr int LDA_T = BK + 4;  // sA[m][k]  (op(A) = A^T)
+constexpr int LDB_N = BK + 8;  // sB[n][k]  (op(B) = B)
+constexpr int LDB_T = BN + 2;  // sB[k][n]  (op(B) = B^T)
+
+template <bool TA>
+__host__ __device__ constexpr int a_elems() {
+  return TA ? BM * LDA_T : BK * LDA_N;
+}
+template <bool TB>
+__host__ __device__ constexpr int b_elems() {
+  return TB ? BK * LDB_T : BN * LDB_N;
+}
+template <bool TA, bool TB>
+constexpr int smem_bytes() {
+  return STAGES * (a_elems<TA>() + b_elems<TB>()) * 8;
+}
+
+struct KParams {
+  GemmArgs g;
+  int tiles_m, tiles_n;
+  int splitk;
+  double* P;  // split-K partials
+  int64_t ldp;
+};
+
+template <bool TA, bool TB, bool V16>
+__global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
+  extern __shared__ __align__(16) double smem[];
+  const GemmArgs& p = kp.g;
+  double* sAb = smem;
+  double* sBb = smem + STAGES * a_elems<TA>();
+
+  const int bz = blockIdx.z;
+  const int split = blockIdx.y;
+  int tm, tn;
+  if (p.tri) {
+    const int t = blockIdx.x;
+    int r = static_cast<int>((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+    while ((r + 1) * (r + 2) / 2 <= t) ++r;
+    while (r * (r + 1) / 2 > t) --r;
+    tm = r;
+    tn = t - r * (r + 1) / 2;
+  } else {
+    const int G = 8;
+    const int t = blockIdx.x;
+    const int group = t / (G * kp.tiles_n);
+    const int first = group * G;
+    const int gsz = min(kp.tiles_m - first, G);
+    const int in = t - group * G * kp.tiles_n;
+    tm = first + in % gsz;
+    tn = in / gsz;
+  }
+  const int m0 = tm * BM, n0 = tn * BN;
+  const int M = p.M, N = p.N;
+
+  int kb = 0, ke = p.K;
+  if (p.kfrom_n) kb = min(n0, ke);
+  if (kp.splitk > 1) {
+    const int span = ke - kb;
+    int len = (span + kp.splitk - 1) / kp.splitk;
+    len = (len + BK - 1) / BK * BK;
+    const int nb = kb + split * len;
+    kb = min(nb, ke);
+    ke = min(nb + len, ke);
+  }
+
+  const double* A = p.A + static_cast<int64_t>(bz) * p.strideA;
+  const double* B = p.B + static_cast<int64_t>(bz) * p.strideB;
+  const int64_t lda = p.lda, ldb = p.ldb;
+  const int tid = threadIdx.x;
+
+  // Each thread moves four 16-byte chunks (two FP64 values along the contiguous
+  // dimension) per operand per stage.  V16: one 16-byte cp.async with zero
+  // fill; otherwise (odd leading dimension / unaligned base) two 8-byte copies.
+  auto chunk = [&](double* dst, const double* base, int64_t off0, bool in0, bool in1, int64_t step) {
+    if (V16) {
+      const int bytes = in0 ? (in1 ? 16 : 8) : 0;
+      cp_async16(dst, bytes ? base + off0 : base, bytes);
+    } else {
+      cp_async8(dst, in0 ? base + off0 : base, in0 ? 8 : 0);
+      cp_async8(dst + 1, in1 ? base + off0 + step : base, in1 ? 8 : 0);
+    }
+  };
+  auto load_stage = [&](int stage, int k0) {
+    double* sa = sAb + stage * a_elems<TA>();
+    double* sb = sBb + stage * b_elems<TB>();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tid + i * NT;
+      if (!TA) {
+        const int k = c >> 6, m = (c & 63) * 2;
+        const int gm = m0 + m, gk = k0 + k;
+        const bool kin = gk < ke;
+        chunk(sa + k * LDA_N + m, A, gm + static_cast<int64_t>(gk) * lda, kin && gm < M, kin && gm + 1 < M, 1);
+      } else {
+        const int m = c >> 3, k = (c & 7) * 2;
+        const int gm = m0 + m, gk = k0 + k;
+        const bool min_ = gm < M;
+        chunk(sa + m * LDA_T + k, A, gk + static_cast<int64_t>(gm) * lda, min_ && gk < ke, min_ && gk + 1 < ke, 1);
+      }
+      if (!TB) {
+        const int n = c >> 3, k = (c & 7) * 2;
+        const int gn = n0 + n, gk = k0 + k;
+        const bool nin = gn < N;
+        chunk(sb + n * LDB_N + k, B, gk + static_cast<int64_t>(gn) * ldb, nin && gk < ke, nin && gk + 1 < ke, 1);
+      } else {
+        const int k = c >> 6, n = (c & 63) * 2;
+        const int gn = n0 + n, gk = k0 + k;
+        const bool kin = gk < ke;
+        chunk(sb + k * LDB_T + n, B, gn + static_cast<int64_t>(gk) * ldb, kin && gn < N, kin && gn + 1 < N, 1);
+      }
+    }
+  };
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 64;
+  const int wn = (warp >> 1) * 32;
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+
+  const int ktiles = (ke > kb) ? (ke - kb + BK - 1) / BK : 0;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles) load_stage(s, kb + s * BK);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < ktiles; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + STAGES - 1;
+      if (nk < ktiles) load_stage(nk % STAGES, kb + nk * BK);
+      cp_async_commit();
+    }
+    const double* sa = sAb + (kt % STAGES) * a_elems<TA>();
+    const double* sb = sBb + (kt % STAGES) * b_elems<TB>();
+#pragma unroll
+    for (int kk = 0; kk < BK / 8; ++kk) {
+      double af[4][4];
+      double bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int m = wm + i * 16 + 2 * g;
+        if (!TA) {
+          const double2 v0 = *reinterpret_cast<const double2*>(sa + (kk * 8 + 2 * t) * LDA_N + m);
+          const double2 v1 = *reinterpret_cast<const double2*>(sa + (kk * 8 + 2 * t + 1) * LDA_N + m);
+          af[i][0] = v0.x;
+          af[i][1] = v0.y;
+          af[i][2] = v1.x;
+          af[i][3] = v1.y;
+        } else {
+          const double2 v0 = *reinterpret_cast<const double2*>(sa + m * LDA_T + kk * 8 + 2 * t);
+          const double2 v1 = *reinterpret_cast<const double2*>(sa + (m + 1) * LDA_T + kk * 8 + 2 * t);
+          af[i][0] = v0.x;
+          af[i][2] = v0.y;
+          af[i][1] = v1.x;
+          af[i][3] = v1.y;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int n = wn + j * 8 + g;
+        if (!TB) {
+          const double2 v = *reinterpret_cast<const double2*>(sb + n * LDB_N + kk * 8 + 2 * t);
+          bf[j][0] = v.x;
+          bf[j][1] = v.y;
+        } else {
+          bf[j][0] = sb[(kk * 8 + 2 * t) * LDB_T + n];
+          bf[j][1] = sb[(kk * 8 + 2 * t + 1) * LDB_T + n];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  // ---- epilogue ----
+  if (kp.splitk > 1) {
+    double* P = kp.P + (static_cast<int64_t>(split) * p.batch + bz) * kp.ldp * N;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = m0 + wm + i * 16 + 2 * g;
+        const int c = n0 + wn + j * 8 + 2 * t;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int cc = c + h;
+          if (cc >= N) continue;
+          double* dst = P + r + static_cast<int64_t>(cc) * kp.ldp;
+          if (r < M) dst[0] = acc[i][j][h];
+          if (r + 1 < M) dst[1] = acc[i][j][2 + h];
+        }
+      }
+    return;
+  }
+  double* C = p.C + static_cast<int64_t>(bz) * p.strideC;
+  const int64_t ldc = p.ldc;
+  const double alpha = p.alpha * (p.alpha_vec ? p.alpha_vec[bz] : 1.0);
+  const double beta = p.beta;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = m0 + wm + i * 16 + 2 * g;
+      const int c = n0 + wn + j * 8 + 2 * t;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int cc = c + h;
+        if (cc >= N || r >= M) continue;
+        double* dst = C + r + static_cast<int64_t>(cc) * ldc;
+        double v0 = alpha * acc[i][j][h];
+        double v1 = alpha * acc[i][j][2 + h];
+        const bool ok0 = !p.tri || r >= cc;
+        const bool ok1 = (r + 1 < M) && (!p.tri || r + 1 >= cc);
+        if (V16 && ok0 && ok1) {
+          if (beta != 0.0) {
+            const double2 o = *reinterpret_cast<const double2*>(dst);
+            v0 += beta * o.x;
+            v1 += beta * o.y;
+          }
+          *reinterpret_cast<double2*>(dst) = make_double2(v0, v1);
+        } else {
+          if (ok0) dst[0] = (beta != 0.0) ? v0 + beta * dst[0] : v0;
+          if (ok1) dst[1] = (beta != 0.0) ? v1 + beta * dst[1] : v1;
+        }
+      }
+    }
+}
+
+__global__ void splitk_reduce_kernel(GemmArgs p, int splitk, const double* P, int64_t ldp) {
+  const int64_t total = static_cast<int64_t>(p.M) * p.N;
+  const int bz = blockIdx.y;
+  const double alpha = p.alpha * (p.alpha_vec ? p.alpha_vec[bz] : 1.0);
+  double* C = p.C + static_cast<int64_t>(bz) * p.strideC;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % p.M);
+    const int j = static_cast<int>(e / p.M);
+    if (p.tri && i < j) continue;
+    double s = 0.0;
+    for (int q = 0; q < splitk; ++q)
+      s += P[(static_cast<int64_t>(q) * p.batch + bz) * ldp * p.N + i + static_cast<int64_t>(j) * ldp];
+    double* dst = C + i + static_cast<int64_t>(j) * p.ldc;
+    double v = alpha * s;
+    if (p.beta != 0.0) v += p.beta * *dst;
+    *dst = v;
+  }
+}
+
+template <bool TA, bool TB, bool V16>
+cudaError_t launch_t(const KParams& kp, dim3 grid, cudaStream_t st) {
+  static bool attr_set = false;
+  constexpr int sm = smem_bytes<TA, TB>();
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<TA, TB, V16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  dgemm_kernel<TA, TB, V16><<<grid, NT, sm, st>>>(kp);
+  return cudaGetLastError();
+}
+
+template <bool V16>
+cudaError_t launch_v(const KParams& kp, dim3 grid, cudaStream_t st) {
+  const GemmArgs& a = kp.g;
+  if (!a.transA && !a.transB) return launch_t<false, false, V16>(kp, grid, st);
+  if (!a.transA && a.transB) return launch_t<false, true, V16>(kp, grid, st);
+  if (a.transA && !a.transB) return launch_t<true, false, V16>(kp, grid, st);
+  return launch_t<true, true, V16>(kp, grid, st);
+}
+
+int choose_splitk(const GemmArgs& a, int sms) {
+  if (a.splitk >= 1) return a.splitk;
+  const int tm = (a.M + BM - 1) / BM, tn = (a.N + BN - 1) / BN;
+  const int64_t tiles = a.tri ? static_cast<int64_t>(tm) * (tm + 1) / 2 : static_cast<int64_t>(tm) * tn;
+  const int64_t ctas = tiles * a.batch;
+  if (ctas >= sms) return 1;
+  const int kt = (a.K + BK - 1) / BK;
+  int s = static_cast<int>((2 * sms + ctas - 1) / ctas);
+  s = std::min(s, kt / 8);
+  s = std::min(s, 32);
+  return std::max(s, 1);
+}
+
+}  // namespace
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+size_t dgemm_splitk_bytes(const GemmArgs& a, int sms) {
+  const int s = choose_splitk(a, sms);
+  if (s <= 1) return 0;
+  const int64_t ldp = (a.M + 1) / 2 * 2;
+  return static_cast<size_t>(s) * a.batch * ldp * a.N * sizeof(double);
+}
+
+cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
+  if (a.M <= 0 || a.N <= 0 || a.batch <= 0) return cudaSuccess;
+  if (a.tri && a.M != a.N) return cudaErrorInvalidValue;
+  // 16-byte cp.async path when every tile chunk is 16-byte aligned, else 8-byte copies
+  auto al = [](const void* ptr, int64_t ld) {
+    return (reinterpret_cast<uintptr_t>(ptr) % 16 == 0) && (ld % 2 == 0);
+  };
+  auto al8 = [](const void* ptr) { return reinterpret_cast<uintptr_t>(ptr) % 8 == 0; };
+  if (!al8(a.A) || !al8(a.B) || !al8(a.C)) return cudaErrorMisalignedAddress;
+  const bool v16 = al(a.A, a.lda) && al(a.B, a.ldb) && al(a.C, a.ldc) &&
+                   (a.batch <= 1 || ((a.strideA | a.strideB | a.strideC) & 1) == 0);
+  const int sms = num_sms();
+  if (a.K <= 0) {
+    // C = beta*C
+    return scale_copy(a.M, a.N, a.beta, a.C, a.ldc, a.strideC, a.C, a.ldc, a.strideC, a.batch, 0.0, st);
+  }
+  KParams kp;
+  kp.g = a;
+  kp.tiles_m = (a.M + BM - 1) / BM;
+  kp.tiles_n = (a.N + BN - 1) / BN;
+  kp.splitk = choose_splitk(a, sms);
+  kp.ldp = (a.M + 1) / 2 * 2;
+  kp.P = nullptr;
+  if (kp.splitk > 1) {
+    const size_t need = static_cast<size_t>(kp.splitk) * a.batch * kp.ldp * a.N * sizeof(double);
+    if (ws.ptr == nullptr || ws.bytes < need) {
+      kp.splitk = 1;  // not enough scratch: run unsplit
+    } else {
+      kp.P = ws.ptr;
+    }
+  }
+  const int64_t tiles = a.tri ? static_cast<int64_t>(kp.tiles_m) * (kp.tiles_m + 1) / 2
+                              : static_cast<int64_t>(kp.tiles_m) * kp.tiles_n;
+  if (tiles > 0x7fffffff || a.batch > 65535) return cudaErrorInvalidValue;
+  dim3 grid(static_cast<unsigned>(tiles), kp.splitk, a.batch);
+  const cudaError_t e = v16 ? launch_v<true>(kp, grid, st) : launch_v<false>(kp, grid, st);
+  if (e != cudaSuccess || kp.splitk <= 1) return e;
+  const int64_t total = static_cast<int64_t>(a.M) * a.N;
+  int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 4 * sms));
+  splitk_reduce_kernel<<<dim3(blocks, a.batch), 256, 0, st>>>(a, kp.splitk, kp.P, kp.ldp);
+  return cudaGetLastError();
+}
+
+}  // namespace zolo

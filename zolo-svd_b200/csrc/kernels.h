@@ -1,0 +1,98 @@
+// Host-side launchers of the FP64 kernels.  Internal to the library (the public
+// C-ABI is include/zolo_b200.h).  All matrices are column-major FP64 in device
+// memory; every launcher takes an explicit stream and returns cudaError_t.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace zolo {
+
+// C(b) = alpha * a_b * op(A(b)) * op(B(b)) + beta * C(b),  b = 0..batch-1
+struct GemmArgs {
+  int M = 0, N = 0, K = 0;
+  int transA = 0, transB = 0;
+  const double* A = nullptr;
+  int64_t lda = 0, strideA = 0;
+  const double* B = nullptr;
+  int64_t ldb = 0, strideB = 0;
+  double* C = nullptr;
+  int64_t ldc = 0, strideC = 0;
+  double alpha = 1.0, beta = 0.0;
+  const double* alpha_vec = nullptr;  // per-batch factor a_b (device), nullptr = 1
+  int batch = 1;
+  int tri = 0;      // 1: M == N, write only C(i,j) with i >= j (lower triangle)
+  int kfrom_n = 0;  // 1: op(B)(k,n) == 0 for k < n (op(B) lower triangular): skip those k
+  int splitk = 0;   // 0 = choose; 1 = off; >1 = number of K slices
+};
+
+// Scratch for split-K partial sums (owned by the caller's context).
+struct Scratch {
+  double* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st);
+size_t dgemm_splitk_bytes(const GemmArgs& a, int num_sms);
+
+// ---- elementwise / reductions (elementwise.cu) ----
+// dst(i,j) = s * src(i,j) (+ d on the diagonal), batched.
+cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, int64_t strideS,
+                       double* dst, int64_t ldd, int64_t strideD, int batch, double diag_add,
+                       cudaStream_t st);
+// W = [X; 0; s I]: X (m x n) in rows [0,m), zeros in [m,mpad), s I in rows [mpad, mpad+n)
+// (mpad >= m keeps the identity block at an even row offset), batched over s_vec[b] or s_scalar.
+cudaError_t form_stack(int m, int mpad, int n, const double* X, int64_t ldx, double* W, int64_t ldw,
+                       int64_t strideW, const double* s_vec, double s_scalar, int batch,
+                       cudaStream_t st);
+// dst(b) = lower(G) + c_b I (lower triangle + diagonal only), batched.
+cudaError_t shift_lower(int n, const double* G, int64_t ldg, double* W, int64_t ldw,
+                        int64_t strideW, const double* c_vec, int batch, cudaStream_t st);
+// Sum of squares partials -> out[0] = ||X||_F^2 (deterministic two-pass).
+cudaError_t frob2(int m, int n, const double* X, int64_t ldx, double* partial, double* out,
+                  cudaStream_t st);
+// out[0] = max_j sum_i |X(i,j)|
+cudaError_t norm1(int m, int n, const double* X, int64_t ldx, double* colsum, double* out,
+                  cudaStream_t st);
+// X <- cx X + sum_q w_q Z_q, w_q = cz_vec[q] (device) or cz; err2 = ||X_new - X_old||_F^2
+// (FormX2 of Zolo-PD with w_q = a_q / FONE, cx = 1/FONE; QDWH update with cx = bkk, cz = akk)
+cudaError_t combine_update(int m, int n, double* X, int64_t ldx, const double* Z, int64_t ldz,
+                           int64_t strideZ, int nz, double cx, double cz, const double* cz_vec,
+                           double* partial, double* err2, cudaStream_t st);
+// H = (B + B^T)/2 (in place on an n x n matrix).
+cudaError_t symmetrize(int n, double* B, int64_t ldb, cudaStream_t st);
+// B = A^T
+cudaError_t transpose(int m, int n, const double* A, int64_t lda, double* B, int64_t ldb,
+                      cudaStream_t st);
+// Q = [I; 0] (m x n, batched)
+cudaError_t set_identity(int m, int n, double* Q, int64_t ldq, int64_t strideQ, int batch,
+                         double diag, cudaStream_t st);
+// A(i,i) += d
+cudaError_t add_diag(int n, double* A, int64_t lda, double d, cudaStream_t st);
+// sum of a device vector of partials into out (helper used by reductions)
+cudaError_t reduce_sum(const double* partial, int count, double* out, cudaStream_t st);
+
+// ---- Cholesky / triangular (potrf.cu) ----
+// In-place lower Cholesky of nb x nb blocks (nb <= 64), batched; info recorded in status[b].
+cudaError_t potrf_leaf(int nb, double* A, int64_t lda, int64_t strideA, int batch, int* info,
+                       int info_offset, cudaStream_t st);
+// In-place inverse of lower-triangular nb x nb blocks (nb <= 64), batched.
+cudaError_t trtri_leaf(int nb, const double* L, int64_t ldl, int64_t strideL, double* Linv,
+                       int64_t ldi, int64_t strideI, int batch, cudaStream_t st);
+
+// ---- Householder QR panel (qr.cu) ----
+// Factor the m x w panel of each batch entry (w <= 32) in place: V below the
+// diagonal (unit diagonal implied), R on/above it, tau[w], T (w x w upper, ldt = w)
+// of the compact WY form I - V T V^T.  Vexp receives V explicitly (m x w, ldv).
+cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, double* tau,
+                     int64_t strideTau, double* T, int64_t strideT, double* Vexp, int64_t ldv,
+                     int64_t strideV, int batch, cudaStream_t st);
+// Vexp = unit-lower-trapezoidal V taken from A (m x w), batched.
+cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t strideA, double* V,
+                      int64_t ldv, int64_t strideV, int batch, cudaStream_t st);
+// P'(b) = T(b)^T * P(b) (trans=1) or T(b) * P(b) (trans=0); T w x w upper (ldt=w), P w x n.
+cudaError_t apply_t(int w, int n, const double* T, int64_t strideT, double* P, int64_t ldp,
+                    int64_t strideP, int trans, int batch, cudaStream_t st);
+
+int num_sms();
+
+}  // namespace zolo

@@ -1,0 +1,150 @@
+// Recursive Cholesky / triangular solves and the blocked structured Householder
+// QR, expressed as DMMA GEMMs plus small leaf kernels.  See linalg.h.
+#include "linalg.h"
+
+#include <algorithm>
+#include <stdexcept>
+
+namespace zolo {
+
+namespace {
+constexpr int NB = 64;  // leaf of the Cholesky / TRSM recursion
+constexpr int PW = 32;  // Householder panel width
+
+int split_point(int n) {
+  int n1 = ((n / 2) + NB - 1) / NB * NB;
+  if (n1 >= n) n1 = n - NB;
+  if (n1 <= 0) n1 = n / 2;
+  return n1;
+}
+}  // namespace
+
+void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
+          int batch, const double* alpha_vec, int tri, int kfrom_n) {
+  GemmArgs a;
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  a.transA = transA;
+  a.transB = transB;
+  a.A = A.p;
+  a.lda = A.ld;
+  a.strideA = A.stride;
+  a.B = B.p;
+  a.ldb = B.ld;
+  a.strideB = B.stride;
+  a.C = C.p;
+  a.ldc = C.ld;
+  a.strideC = C.stride;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.alpha_vec = alpha_vec;
+  a.batch = batch;
+  a.tri = tri;
+  a.kfrom_n = kfrom_n;
+  const size_t need = dgemm_splitk_bytes(a, num_sms());
+  if (need) c.ensure_splitk(need);
+  ck(dgemm(a, c.splitk(), c.stream()));
+  c.stats.launches += need ? 2 : 1;
+}
+
+static void potrf_rec(Context& c, int n, Mat A, int batch, int* dinfo, int off) {
+  if (n <= NB) {
+    ck(potrf_leaf(n, A.p, A.ld, A.stride, batch, dinfo, off, c.stream()));
+    c.stats.launches++;
+    return;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  potrf_rec(c, n1, A, batch, dinfo, off);
+  // A21 <- A21 L11^{-T}
+  const int64_t ldt = (n2 + 1) / 2 * 2;
+  Mat tmp{c.buf("potrf_tmp", static_cast<size_t>(ldt) * n1 * batch), ldt, ldt * n1};
+  ck(scale_copy(n2, n1, 1.0, A.at(n1, 0).p, A.ld, A.stride, tmp.p, tmp.ld, tmp.stride, batch, 0.0, c.stream()));
+  c.stats.launches++;
+  trsm_rlt(c, n2, n1, A, tmp, A.at(n1, 0), batch);
+  // A22 -= A21 A21^T (lower)
+  gemm(c, 0, 1, n2, n2, n1, -1.0, A.at(n1, 0), A.at(n1, 0), 1.0, A.at(n1, n1), batch, nullptr, 1, 0);
+  potrf_rec(c, n2, A.at(n1, n1), batch, dinfo, off + n1);
+}
+
+void potrf(Context& c, int n, Mat A, int batch, int* dinfo) { potrf_rec(c, n, A, batch, dinfo, 0); }
+
+void trsm_rlt(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch) {
+  if (n <= NB) {
+    Mat li{c.buf("trsm_linv", static_cast<size_t>(NB) * NB * batch), NB, NB * NB};
+    ck(trtri_leaf(n, L.p, L.ld, L.stride, li.p, li.ld, li.stride, batch, c.stream()));
+    c.stats.launches++;
+    gemm(c, 0, 1, m, n, n, 1.0, X, li, 0.0, Y, batch);
+    return;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  trsm_rlt(c, m, n1, L, X, Y, batch);
+  gemm(c, 0, 1, m, n2, n1, -1.0, Y, L.at(n1, 0), 1.0, X.at(0, n1), batch);
+  trsm_rlt(c, m, n2, L.at(n1, n1), X.at(0, n1), Y.at(0, n1), batch);
+}
+
+void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch) {
+  if (n <= NB) {
+    Mat li{c.buf("trsm_linv", static_cast<size_t>(NB) * NB * batch), NB, NB * NB};
+    ck(trtri_leaf(n, L.p, L.ld, L.stride, li.p, li.ld, li.stride, batch, c.stream()));
+    c.stats.launches++;
+    gemm(c, 0, 0, m, n, n, 1.0, X, li, 0.0, Y, batch);
+    return;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  trsm_rln(c, m, n2, L.at(n1, n1), X.at(0, n1), Y.at(0, n1), batch);
+  gemm(c, 0, 0, m, n1, n2, -1.0, Y.at(0, n1), L.at(n1, 0), 1.0, X, batch);
+  trsm_rln(c, m, n1, L, X, Y, batch);
+}
+
+static inline int row_hi(int mtot, int m_top, int j, int jb) {
+  return m_top >= 0 ? std::min(mtot, m_top + j + jb) : mtot;
+}
+
+void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch) {
+  const int npan = (n + PW - 1) / PW;
+  const int64_t ldv = (mtot + 1) / 2 * 2;
+  Mat V{c.buf("qr_v", static_cast<size_t>(ldv) * PW * batch), ldv, ldv * PW};
+  Mat P{c.buf("qr_p", static_cast<size_t>(PW) * n * batch), PW, static_cast<int64_t>(PW) * n};
+  const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
+  for (int j = 0; j < n; j += PW) {
+    const int jb = std::min(PW, n - j);
+    const int rhi = row_hi(mtot, m_top, j, jb);
+    const int mp = rhi - j;
+    ck(qr_panel(mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + (j / PW) * PW * PW, strideT, V.p, V.ld,
+                V.stride, batch, c.stream()));
+    c.stats.launches++;
+    const int nc = n - j - jb;
+    if (nc > 0) {
+      gemm(c, 1, 0, jb, nc, mp, 1.0, V, W.at(j, j + jb), 0.0, P, batch);
+      ck(apply_t(jb, nc, T + (j / PW) * PW * PW, strideT, P.p, P.ld, P.stride, 1, batch, c.stream()));
+      c.stats.launches++;
+      gemm(c, 0, 0, mp, nc, jb, -1.0, V, P, 1.0, W.at(j, j + jb), batch);
+    }
+  }
+}
+
+void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch) {
+  const int npan = (n + PW - 1) / PW;
+  const int64_t ldv = (mtot + 1) / 2 * 2;
+  Mat V{c.buf("qr_v", static_cast<size_t>(ldv) * PW * batch), ldv, ldv * PW};
+  Mat P{c.buf("qr_p", static_cast<size_t>(PW) * n * batch), PW, static_cast<int64_t>(PW) * n};
+  const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
+  ck(set_identity(mtot, n, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
+  c.stats.launches++;
+  for (int pj = npan - 1; pj >= 0; --pj) {
+    const int j = pj * PW;
+    const int jb = std::min(PW, n - j);
+    const int rhi = row_hi(mtot, m_top, j, jb);
+    const int mp = rhi - j;
+    const int nc = n - j;
+    ck(extract_v(mp, jb, W.at(j, j).p, W.ld, W.stride, V.p, V.ld, V.stride, batch, c.stream()));
+    c.stats.launches++;
+    gemm(c, 1, 0, jb, nc, mp, 1.0, V, Q.at(j, j), 0.0, P, batch);
+    ck(apply_t(jb, nc, T + pj * PW * PW, strideT, P.p, P.ld, P.stride, 0, batch, c.stream()));
+    c.stats.launches++;
+    gemm(c, 0, 0, mp, nc, jb, -1.0, V, P, 1.0, Q.at(j, j), batch);
+  }
+}
+
+}  // namespace zolo

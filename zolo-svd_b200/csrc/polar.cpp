@@ -1,0 +1,379 @@
+// QDWH-PD (pqdwhfacs.f90:296-466, zolopd.f90:290-440) and Zolo-PD
+// (pzolopd1.f90:280-487) on one GPU.  The iteration control is host scalar
+// code identical to the reference; every matrix operation is one of the FP64
+// kernels.  In Zolo-PD the r independent Zolotarev terms of an iteration are
+// batched into the same launches (the reference runs them on r process
+// groups and sums them with DGSUM2D); the sum is fused into the FormX2 kernel.
+#include "polar.h"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "coeff.h"
+#include "linalg.h"
+
+namespace zolo {
+
+namespace {
+
+inline int64_t even(int64_t x) { return (x + 1) / 2 * 2; }
+
+double d2h(Context& c, const double* d) {
+  double v = 0.0;
+  ck(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  return v;
+}
+
+void h2d(Context& c, double* d, const double* h, int n) {
+  ck(cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, c.stream()));
+}
+
+int read_info(Context& c, int* dinfo, int count) {
+  std::vector<int> h(count, 0);
+  ck(cudaMemcpyAsync(h.data(), dinfo, count * sizeof(int), cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  for (int v : h)
+    if (v != 0) return v;
+  return 0;
+}
+
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    ck(cudaEventCreate(&a));
+    ck(cudaEventCreate(&b));
+    ck(cudaEventRecord(a, s));
+  }
+  double stop() {
+    ck(cudaEventRecord(b, s));
+    ck(cudaEventSynchronize(b));
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+  ~EventTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+int npanels(int n) { return (n + 31) / 32; }
+
+// Q1 * Q2^T of the explicit Q of the stacked matrix (Q2 starts at row mp, upper triangular).
+void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
+  gemm(c, 0, 1, m, n, n, 1.0, Qf, Qf.at(mp, 0), 0.0, Z, batch, nullptr, 0, 1);
+}
+
+// Z(b) = X W_b^{-1} (left = false) or W_b^{-1} X (left = true, square X), W_b = L_b L_b^T.
+void spd_solve(Context& c, int m, int n, const double* X, int64_t ldx, Mat Lw, Mat Z, int batch, bool left) {
+  const int64_t ldm = even(m);
+  Mat Xc{c.buf("Xc", static_cast<size_t>(ldm) * n * batch), ldm, ldm * n};
+  Mat Y{c.buf("Y", static_cast<size_t>(ldm) * n * batch), ldm, ldm * n};
+  if (!left) {
+    ck(scale_copy(m, n, 1.0, X, ldx, 0, Xc.p, Xc.ld, Xc.stride, batch, 0.0, c.stream()));
+    c.stats.launches++;
+    trsm_rlt(c, m, n, Lw, Xc, Y, batch);
+    trsm_rln(c, m, n, Lw, Y, Z, batch);
+    return;
+  }
+  // W^{-1} X = (X^T W^{-1})^T : transpose in, right solves, transpose out
+  for (int b = 0; b < batch; ++b) {
+    ck(transpose(m, n, X, ldx, Xc.p + b * Xc.stride, Xc.ld, c.stream()));
+    c.stats.launches++;
+  }
+  trsm_rlt(c, n, m, Lw, Xc, Y, batch);
+  trsm_rln(c, n, m, Lw, Y, Xc, batch);
+  for (int b = 0; b < batch; ++b) {
+    ck(transpose(n, m, Xc.p + b * Xc.stride, Xc.ld, Z.p + b * Z.stride, Z.ld, c.stream()));
+    c.stats.launches++;
+  }
+}
+
+}  // namespace
+
+void form_h(Context& c, int m, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, double* dH,
+            int64_t ldh) {
+  const int64_t ldn = even(n);
+  double* Hb = c.buf("Hbuf", static_cast<size_t>(ldn) * n);
+  gemm(c, 1, 0, n, n, m, 1.0, Mat{const_cast<double*>(dQ), ldq, 0}, Mat{const_cast<double*>(dA), lda, 0}, 0.0,
+       Mat{Hb, ldn, 0}, 1);
+  ck(symmetrize(n, Hb, ldn, c.stream()));
+  ck(scale_copy(n, n, 1.0, Hb, ldn, 0, dH, ldh, 0, 1, 0.0, c.stream()));
+  c.stats.launches += 2;
+  c.stats.flops += 2.0 * m * static_cast<double>(n) * n;
+}
+
+int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda, BoundsMode mode, double* alpha,
+           double* beta) {
+  const int64_t ldx = even(m), ldn = even(n);
+  double* X = c.buf("bnd_x", static_cast<size_t>(ldx) * n);
+  double* scal = c.dscal();
+  double* part = c.dpartial();
+  ck(scale_copy(m, n, 1.0, dA, lda, 0, X, ldx, 0, 1, -sigma, c.stream()));
+  ck(frob2(m, n, X, ldx, part, scal, c.stream()));
+  c.stats.launches += 3;
+  const double a = std::sqrt(d2h(c, scal));
+  *alpha = a;
+  if (!(a > 0.0) || !std::isfinite(a)) {
+    *beta = 0.0;
+    return 1;
+  }
+  ck(scale_copy(m, n, 1.0 / a, X, ldx, 0, X, ldx, 0, 1, 0.0, c.stream()));
+  c.stats.launches++;
+  double temp_beta = 1.0;
+  if (mode == BOUNDS_PQDWHFACS) {
+    double* colsum = c.buf("bnd_colsum", n);
+    ck(norm1(m, n, X, ldx, colsum, scal + 1, c.stream()));
+    c.stats.launches += 2;
+    temp_beta = d2h(c, scal + 1);
+  }
+  // R of X = QR (unstructured Householder), then ||R^{-1}||_1 from R^{-1} = I * (R^T)^{-T}
+  double* tau = c.buf("bnd_tau", n);
+  double* T = c.buf("bnd_t", static_cast<size_t>(npanels(n)) * 1024);
+  geqrf(c, m, n, -1, Mat{X, ldx, 0}, tau, T, 1);
+  double* Lt = c.buf("bnd_lt", static_cast<size_t>(ldn) * n);
+  double* I = c.buf("bnd_i", static_cast<size_t>(ldn) * n);
+  double* Ri = c.buf("bnd_rinv", static_cast<size_t>(ldn) * n);
+  ck(transpose(n, n, X, ldx, Lt, ldn, c.stream()));
+  ck(set_identity(n, n, I, ldn, 0, 1, 1.0, c.stream()));
+  c.stats.launches += 2;
+  trsm_rlt(c, n, n, Mat{Lt, ldn, 0}, Mat{I, ldn, 0}, Mat{Ri, ldn, 0}, 1);
+  double* colsum = c.buf("bnd_colsum", n);
+  ck(norm1(n, n, Ri, ldn, colsum, scal + 2, c.stream()));
+  ck(frob2(n, n, Ri, ldn, part, scal + 3, c.stream()));
+  c.stats.launches += 4;
+  const double inv1 = d2h(c, scal + 2);
+  const double fr = d2h(c, scal + 3);
+  c.stats.flops += 4.0 / 3.0 * static_cast<double>(n) * n * n + 2.0 * m * static_cast<double>(n) * n;
+  if (!std::isfinite(fr) || !std::isfinite(inv1) || !(inv1 > 0.0)) {
+    *beta = 0.0;
+    return 1;
+  }
+  *beta = temp_beta / (std::sqrt(static_cast<double>(n)) * inv1);
+  return 0;
+}
+
+int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh,
+         const QdwhOpts& o) {
+  if (m < n) return -1;
+  if (m == 0 || n == 0) return 0;
+  c.stats = Stats{};
+  EventTimer total(c.stream());
+  // internal copies with an even leading dimension (16-byte aligned GEMM tiles)
+  const int64_t ldx = even(m);
+  double* Ain = c.buf("Ain", static_cast<size_t>(ldx) * n);
+  double* X = c.buf("Xit", static_cast<size_t>(ldx) * n);
+  ck(scale_copy(m, n, 1.0, dA, lda, 0, Ain, ldx, 0, 1, 0.0, c.stream()));
+  c.stats.launches++;
+  double alpha = 0, beta = 0;
+  {
+    EventTimer tb(c.stream());
+    const int info = bounds(c, m, n, o.sigma, Ain, ldx, o.bounds, &alpha, &beta);
+    c.stats.ms_bounds = tb.stop();
+    c.stats.alpha = alpha;
+    c.stats.beta = beta;
+    if (info != 0) {
+      c.stats.info = info;
+      return info;
+    }
+  }
+  ck(scale_copy(m, n, 1.0, Ain, ldx, 0, X, ldx, 0, 1, -o.sigma, c.stream()));
+  ck(scale_copy(m, n, 1.0 / alpha, X, ldx, 0, X, ldx, 0, 1, 0.0, c.stream()));
+  c.stats.launches += 2;
+
+  const double eps = eps_precision();
+  const double tol1 = 10.0 * eps / 2.0;
+  const double tol2 = std::exp(std::log(tol1) / 3.0);
+  const int mp = static_cast<int>(even(m));  // row offset of the sqrt(c) I block in the stack
+  const int64_t ldw = even(static_cast<int64_t>(mp) + n), ldz = even(m), ldn = even(n);
+  Mat W{c.buf("W", static_cast<size_t>(ldw) * n), ldw, 0};
+  Mat Qf{c.buf("Qf", static_cast<size_t>(ldw) * n), ldw, 0};
+  Mat Z{c.buf("Z", static_cast<size_t>(ldz) * n), ldz, 0};
+  Mat G{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
+  double* tau = c.buf("tau", n);
+  double* T = c.buf("qr_t", static_cast<size_t>(npanels(n)) * 1024);
+  int* dinfo = c.dinfo();
+  double* scal = c.dscal();
+  double* part = c.dpartial();
+  const bool left = (o.left_solve || o.sym == 'S' || o.sym == 's') && m == n;
+
+  EventTimer ti(c.stream());
+  double lowk = beta, err = 1.0, err2 = std::fabs(1.0 - lowk);
+  int it = 0;
+  while ((it == 0 || err > tol2 || err2 > tol1) && (o.maxit < 0 || it <= o.maxit) && it < 100) {
+    double ak, bk, ckk, lnext;
+    qdwh_weights(lowk, &ak, &bk, &ckk, &lnext);
+    lowk = lnext;
+    double akk, bkk;
+    bool use_qr = ckk > 100.0;
+    if (!use_qr) {
+      gemm(c, 1, 0, n, n, m, ckk, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+      ck(add_diag(n, G.p, G.ld, 1.0, c.stream()));
+      ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
+      c.stats.launches += 2;
+      potrf(c, n, G, 1, dinfo);
+      const int pinfo = read_info(c, dinfo, 1);
+      if (pinfo != 0) {
+        // not numerically SPD: redo this step with the QR form (the reference ignores PDPOSV's INFO)
+        if (c.stats.info == 0) c.stats.info = pinfo;
+        use_qr = true;
+      } else {
+        spd_solve(c, m, n, X, ldx, G, Z, 1, left);
+        akk = ak - bk / ckk;
+        bkk = bk / ckk;
+        c.stats.chol_iterations++;
+        if (it < 16) c.stats.branch[it] = 2;
+        c.stats.flops += 2.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n / 3.0 +
+                         static_cast<double>(m) * n * n;
+      }
+    }
+    if (use_qr) {
+      const double sck = std::sqrt(ckk);
+      ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, 0, nullptr, 1.0 / sck, 1, c.stream()));
+      c.stats.launches++;
+      geqrf(c, mp + n, n, mp, W, tau, T, 1);
+      orgqr(c, mp + n, n, mp, W, T, Qf, 1);
+      q1q2t(c, m, mp, n, Qf, Z, 1);
+      akk = (ak - bk / ckk) / sck;
+      bkk = bk / ckk;
+      c.stats.qr_iterations++;
+      if (it < 16) c.stats.branch[it] = 1;
+      c.stats.flops += 4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n;
+    }
+    ck(combine_update(m, n, X, ldx, Z.p, Z.ld, 0, 1, bkk, akk, nullptr, part, scal, c.stream()));
+    c.stats.launches += 2;
+    err = std::sqrt(d2h(c, scal));
+    if (it < 16) {
+      c.stats.con[it] = ckk;
+      c.stats.err[it] = err;
+    }
+    ++it;
+    err2 = std::fabs(1.0 - lowk);
+  }
+  c.stats.ms_iter = ti.stop();
+  c.stats.iterations = it;
+  c.stats.last_err = err;
+  ck(scale_copy(m, n, 1.0, X, ldx, 0, dQ, ldq, 0, 1, 0.0, c.stream()));
+  c.stats.launches++;
+  if (dH) {
+    EventTimer th(c.stream());
+    form_h(c, m, n, X, ldx, Ain, ldx, dH, ldh);
+    c.stats.ms_h = th.stop();
+  }
+  c.stats.ms_total = total.stop();
+  return 0;
+}
+
+int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double beta, const double* dA, int64_t lda,
+            double* dQ, int64_t ldq, double* dH, int64_t ldh, int maxit) {
+  if (m < n) return -3;
+  if (rk < 1 || rk > 8) return -2;
+  if (m == 0 || n == 0) return 0;
+  if (!(alpha > 0.0) || !(beta > 0.0)) return -5;
+  c.stats = Stats{};
+  c.stats.alpha = alpha;
+  c.stats.beta = beta;
+  EventTimer total(c.stream());
+  const int64_t ldx = even(m);
+  double* X = c.buf("Xit", static_cast<size_t>(ldx) * n);
+  ck(scale_copy(m, n, 1.0 / (alpha * beta), dA, lda, 0, X, ldx, 0, 1, 0.0, c.stream()));
+  c.stats.launches++;
+
+  const double eps = eps_precision();
+  const double tol = eps;
+  const double tol1 = 10.0 * eps / 2.0;
+  const double tol2 = std::exp(std::log(tol1) / (2.0 * rk + 1.0));
+  const int mp = static_cast<int>(even(m));  // row offset of the sqrt(c) I block in the stack
+  const int64_t ldw = even(static_cast<int64_t>(mp) + n), ldz = even(m), ldn = even(n);
+  const int64_t sW = ldw * n, sZ = ldz * n;
+  Mat W{c.buf("W", static_cast<size_t>(sW) * rk), ldw, sW};
+  Mat Qf{c.buf("Qf", static_cast<size_t>(sW) * rk), ldw, sW};
+  Mat Z{c.buf("Z", static_cast<size_t>(sZ) * rk), ldz, sZ};
+  Mat G{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
+  Mat Wc{W.p, ldn, ldn * n};  // shifted Gram matrices reuse the QR workspace
+  double* tau = c.buf("tau", static_cast<size_t>(n) * rk);
+  double* T = c.buf("qr_t", static_cast<size_t>(npanels(n)) * 1024 * rk);
+  double* dvec = c.buf("zolo_vec", 64);
+  int* dinfo = c.dinfo();
+  double* scal = c.dscal();
+  double* part = c.dpartial();
+  const bool left = (sym == 'S' || sym == 's') && m == n;
+
+  std::vector<double> coeff(3 * rk), hv(64, 0.0);
+  double con = 1.0 / beta, err = 1.0;
+  int it = 0;
+  EventTimer ti(c.stream());
+  while (err > tol2 && it < maxit) {
+    compute_coeff(con, tol, rk, coeff.data());
+    double maxc = coeff[0];
+    for (int i = 1; i < 2 * rk; ++i) maxc = std::max(maxc, coeff[i]);
+    bool use_qr = (it == 0 || con > 1.0e3) && maxc > 3.0e2;
+    if (!use_qr) {
+      gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+      for (int b = 0; b < rk; ++b) hv[b] = coeff[2 * b];
+      h2d(c, dvec, hv.data(), rk);
+      ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk, c.stream()));
+      ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * rk, c.stream()));
+      c.stats.launches += 2;
+      potrf(c, n, Wc, rk, dinfo);
+      const int pinfo = read_info(c, dinfo, rk);
+      if (pinfo != 0) {
+        if (c.stats.info == 0) c.stats.info = pinfo;
+        use_qr = true;  // fall back to the QR form for this step
+      } else {
+        spd_solve(c, m, n, X, ldx, Wc, Z, rk, left);
+        for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b];
+        c.stats.chol_iterations++;
+        if (it < 16) c.stats.branch[it] = 2;
+        c.stats.flops += static_cast<double>(m) * n * n +
+                         rk * (static_cast<double>(n) * n * n / 3.0 + 2.0 * m * static_cast<double>(n) * n);
+      }
+    }
+    if (use_qr) {
+      for (int b = 0; b < rk; ++b) hv[b] = std::sqrt(coeff[2 * b]);
+      h2d(c, dvec, hv.data(), rk);
+      ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk, c.stream()));
+      c.stats.launches++;
+      geqrf(c, mp + n, n, mp, W, tau, T, rk);
+      orgqr(c, mp + n, n, mp, W, T, Qf, rk);
+      q1q2t(c, m, mp, n, Qf, Z, rk);
+      for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b] / std::sqrt(coeff[2 * b]);
+      c.stats.qr_iterations++;
+      if (it < 16) c.stats.branch[it] = 1;
+      c.stats.flops += rk * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
+    }
+    const double fone = zolo_fone(coeff.data(), rk);
+    const double con_next = zolo_next_con(con, coeff.data(), rk, fone);
+    for (int b = 0; b < rk; ++b) hv[16 + b] /= fone;
+    h2d(c, dvec + 16, hv.data() + 16, rk);
+    ck(combine_update(m, n, X, ldx, Z.p, Z.ld, Z.stride, rk, 1.0 / fone, 0.0, dvec + 16, part, scal, c.stream()));
+    c.stats.launches += 2;
+    err = std::sqrt(d2h(c, scal));
+    if (it < 16) {
+      c.stats.con[it] = con;
+      c.stats.err[it] = err;
+    }
+    con = con_next;
+    ++it;
+  }
+  c.stats.ms_iter = ti.stop();
+  c.stats.iterations = it;
+  c.stats.last_err = err;
+  ck(scale_copy(m, n, 1.0, X, ldx, 0, dQ, ldq, 0, 1, 0.0, c.stream()));
+  c.stats.launches++;
+  if (dH) {
+    EventTimer th(c.stream());
+    const int64_t lda_i = even(m);
+    double* Ain = c.buf("Ain", static_cast<size_t>(lda_i) * n);
+    ck(scale_copy(m, n, 1.0, dA, lda, 0, Ain, lda_i, 0, 1, 0.0, c.stream()));
+    form_h(c, m, n, X, ldx, Ain, lda_i, dH, ldh);
+    c.stats.ms_h = th.stop();
+  }
+  c.stats.ms_total = total.stop();
+  return 0;
+}
+
+}  // namespace zolo
