@@ -65,6 +65,12 @@ int zolo_get_stats(zolo_handle_t handle, zolo_stats_t* out);
 int zolo_default_handle(zolo_handle_t* handle);
 int zolo_release_workspace(zolo_handle_t handle);
 const char* zolo_version(void);
+/* Per-kernel-class device timing with CUDA events on the launching streams
+ * (class 0 = DMMA GEMM, 1 = Householder panel, 2 = Cholesky leaf).  While enabled,
+ * zolo_profile_read returns, per class, {launches, milliseconds, algorithmic flops}
+ * accumulated since the last reset (out[3*cls + 0..2]). */
+int zolo_profile_enable(zolo_handle_t handle, int on);
+int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
 
 /* ---- host scalar routines (no GPU needed) ---- */
 /* Compute_Coeff (Auxil_Zolo.f90:165-200): coeff[0:2rk] = c_i, coeff[2rk:3rk] = -a_i. */

@@ -68,6 +68,8 @@ _SIGS = [
     ("zolo_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("zolo_default_handle", C.c_int, [C.POINTER(C.c_void_p)]),
     ("zolo_release_workspace", C.c_int, [C.c_void_p]),
+    ("zolo_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("zolo_profile_read", C.c_int, [C.c_void_p, c_double_p, C.c_int]),
     ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_mellipke", None, [C.c_double, C.c_double, c_double_p, c_double_p]),
     ("zolo_mellipj", None, [C.c_double, C.c_double, C.c_double, c_double_p, c_double_p, c_double_p]),
@@ -280,6 +282,17 @@ class Handle:
 
     def release(self):
         lib().zolo_release_workspace(self.ptr)
+
+    def profile(self, on: bool = True):
+        lib().zolo_profile_enable(self.ptr, 1 if on else 0)
+
+    def profile_read(self, reset: bool = True) -> dict:
+        """Per kernel class: launches, device ms (CUDA events) and algorithmic flops."""
+        out = np.zeros(9)
+        lib().zolo_profile_read(self.ptr, _dp(out), 1 if reset else 0)
+        names = ["dgemm", "qr_panel", "potrf_leaf"]
+        return {nm: dict(launches=int(out[3 * i]), ms=float(out[3 * i + 1]), flops=float(out[3 * i + 2]))
+                for i, nm in enumerate(names)}
 
 
 def colmajor_to_device(a: np.ndarray, device="cuda"):

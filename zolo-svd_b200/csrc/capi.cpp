@@ -210,6 +210,26 @@ int zolo_release_workspace(zolo_handle_t h) {
   });
 }
 
+int zolo_profile_enable(zolo_handle_t h, int on) {
+  return guarded(h, [&](Context& c) {
+    c.prof.on = on != 0;
+    return 0;
+  });
+}
+
+int zolo_profile_read(zolo_handle_t h, double* out, int reset) {
+  return guarded(h, [&](Context& c) {
+    c.prof.collect();
+    for (int k = 0; k < zolo::Profiler::kClasses; ++k) {
+      out[3 * k] = c.prof.launches[k];
+      out[3 * k + 1] = c.prof.ms[k];
+      out[3 * k + 2] = c.prof.flops[k];
+    }
+    if (reset) c.prof.reset();
+    return 0;
+  });
+}
+
 int zolo_get_stats(zolo_handle_t h, zolo_stats_t* out) {
   if (!h || !out) return -2;
   std::lock_guard<std::mutex> lk(h->ctx.mu);
@@ -361,7 +381,8 @@ int zolo_dpotrf_dev(zolo_handle_t h, int n, double* dA, int64_t lda) {
   return guarded(h, [&](Context& c) {
     int* dinfo = c.dinfo();
     zolo::ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
-    zolo::potrf(c, n, zolo::Mat{dA, lda, 0}, 1, dinfo);
+    zolo::DiagInv D{c.buf("dinv", static_cast<size_t>(zolo::nblocks(n)) * 4096), 0};
+    zolo::potrf(c, n, zolo::Mat{dA, lda, 0}, 1, dinfo, D);
     int info = 0;
     zolo::ck(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c.stream()));
     zolo::ck(cudaStreamSynchronize(c.stream()));
@@ -373,8 +394,10 @@ int zolo_dtrsm_dev(zolo_handle_t h, char trans, int m, int n, const double* dL, 
                    double* dY, int64_t ldy) {
   return guarded(h, [&](Context& c) {
     zolo::Mat L{const_cast<double*>(dL), ldl, 0}, X{dX, ldx, 0}, Y{dY, ldy, 0};
-    if (upper(trans)) zolo::trsm_rlt(c, m, n, L, X, Y, 1);
-    else zolo::trsm_rln(c, m, n, L, X, Y, 1);
+    zolo::DiagInv D{c.buf("dinv", static_cast<size_t>(zolo::nblocks(n)) * 4096), 0};
+    zolo::diag_inverses(c, n, L, 1, D);
+    if (upper(trans)) zolo::trsm_rlt(c, m, n, L, X, Y, 1, D);
+    else zolo::trsm_rln(c, m, n, L, X, Y, 1, D);
     zolo::ck(cudaStreamSynchronize(c.stream()));
     return 0;
   });
@@ -431,10 +454,11 @@ int zolo_zolochol_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t l
     zolo::ck(zolo::add_diag(n, G.p, G.ld, cc, c.stream()));
     int* dinfo = c.dinfo();
     zolo::ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
-    zolo::potrf(c, n, G, 1, dinfo);
+    zolo::DiagInv D{c.buf("dinv", static_cast<size_t>(zolo::nblocks(n)) * 4096), 0};
+    zolo::potrf(c, n, G, 1, dinfo, D);
     zolo::ck(zolo::scale_copy(m, n, a, dX, ldx, 0, Xc.p, Xc.ld, 0, 1, 0.0, c.stream()));
-    zolo::trsm_rlt(c, m, n, G, Xc, Y, 1);
-    zolo::trsm_rln(c, m, n, G, Y, zolo::Mat{dZ, ldz, 0}, 1);
+    zolo::trsm_rlt(c, m, n, G, Xc, Y, 1, D);
+    zolo::trsm_rln(c, m, n, G, Y, zolo::Mat{dZ, ldz, 0}, 1, D);
     int info = 0;
     zolo::ck(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, c.stream()));
     zolo::ck(cudaStreamSynchronize(c.stream()));

@@ -6,15 +6,23 @@ Context::Context(int device) : device_(device) {
   ck(cudaSetDevice(device));
   ck(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
   stream_ = own_stream_;
+  int lo = 0, hi = 0;
+  ck(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  ck(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, hi));
+  for (auto& e : ev_) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
 
 Context::~Context() {
   release_all();
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (side_) cudaStreamDestroy(side_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
 void Context::release_all() {
   if (stream_) cudaStreamSynchronize(stream_);
+  if (side_) cudaStreamSynchronize(side_);
   for (auto& kv : bufs_) cudaFree(kv.second.first);
   bufs_.clear();
   if (splitk_.ptr) cudaFree(splitk_.ptr);
@@ -58,6 +66,57 @@ void Context::ensure_splitk(size_t bytes) {
   ck(cudaMalloc(&p, bytes));
   splitk_.ptr = static_cast<double*>(p);
   splitk_.bytes = bytes;
+}
+
+cudaEvent_t Profiler::take() {
+  if (!pool.empty()) {
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  ck(cudaEventCreate(&e));
+  return e;
+}
+
+void Profiler::begin(int cls, double fl, cudaStream_t st, Rec* r) {
+  r->a = take();
+  r->b = take();
+  r->cls = cls;
+  r->flops = fl;
+  ck(cudaEventRecord(r->a, st));
+}
+
+void Profiler::end(Rec& r, cudaStream_t st) {
+  ck(cudaEventRecord(r.b, st));
+  recs.push_back(r);
+}
+
+void Profiler::collect() {
+  for (auto& r : recs) {
+    ck(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    ck(cudaEventElapsedTime(&t, r.a, r.b));
+    launches[r.cls] += 1;
+    ms[r.cls] += t;
+    flops[r.cls] += r.flops;
+    pool.push_back(r.a);
+    pool.push_back(r.b);
+  }
+  recs.clear();
+}
+
+void Profiler::reset() {
+  collect();
+  for (int i = 0; i < kClasses; ++i) launches[i] = ms[i] = flops[i] = 0;
+}
+
+Profiler::~Profiler() {
+  for (auto& r : recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : pool) cudaEventDestroy(e);
 }
 
 double* Context::dscal() { return buf("__scal", 64); }

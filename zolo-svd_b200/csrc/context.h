@@ -6,6 +6,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "kernels.h"
 
@@ -25,6 +26,27 @@ struct Stats {
   int branch[16] = {0};  // 1 = QR, 2 = Cholesky
 };
 
+// Optional per-kernel-class timing with CUDA events recorded around launches on
+// their own stream (class 0 = DMMA GEMM, 1 = Householder panel, 2 = Cholesky leaf).
+struct Profiler {
+  static constexpr int kClasses = 3;
+  bool on = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    int cls;
+    double flops;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double launches[kClasses] = {0, 0, 0}, ms[kClasses] = {0, 0, 0}, flops[kClasses] = {0, 0, 0};
+  cudaEvent_t take();
+  void begin(int cls, double fl, cudaStream_t st, Rec* r);
+  void end(Rec& r, cudaStream_t st);
+  void collect();  // synchronizes the recorded events and folds them into the totals
+  void reset();
+  ~Profiler();
+};
+
 // Thrown inside the library on a CUDA error; converted to an INFO code at the C-ABI.
 struct CudaFailure {
   cudaError_t err;
@@ -42,6 +64,9 @@ class Context {
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  // high-priority stream for latency-bound work overlapped with the main stream
+  cudaStream_t side_stream() const { return side_; }
+  cudaEvent_t event(int i) const { return ev_[i]; }
 
   // Named cached device buffer of at least `elems` doubles (grow-only).
   double* buf(const std::string& name, size_t elems);
@@ -51,6 +76,7 @@ class Context {
   void release_all();
 
   Stats stats;
+  Profiler prof;
   std::mutex mu;
 
   // small device scalars / partial sums
@@ -60,7 +86,8 @@ class Context {
 
  private:
   int device_;
-  cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+  cudaStream_t stream_ = nullptr, own_stream_ = nullptr, side_ = nullptr;
+  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   std::map<std::string, std::pair<void*, size_t>> bufs_;
   Scratch splitk_;
 };

@@ -21,24 +21,25 @@ namespace zolo {
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, NT = 256;
-constexpr int LDA_N = BM + 2;  // sA[k][m]  (op(A) = A)
+constexpr int BK = 16, STAGES = 4, NT = 256;
 constexpr int LDA_T = BK + 4;  // sA[m][k]  (op(A) = A^T)
 constexpr int LDB_N = BK + 8;  // sB[n][k]  (op(B) = B)
-constexpr int LDB_T = BN + 2;  // sB[k][n]  (op(B) = B^T)
 
-template <bool TA>
-__host__ __device__ constexpr int a_elems() {
-  return TA ? BM * LDA_T : BK * LDA_N;
-}
-template <bool TB>
-__host__ __device__ constexpr int b_elems() {
-  return TB ? BK * LDB_T : BN * LDB_N;
-}
-template <bool TA, bool TB>
-constexpr int smem_bytes() {
-  return STAGES * (a_elems<TA>() + b_elems<TB>()) * 8;
-}
+// CTA tile BM x BN, WM x WN warps, each warp owns (BM/WM) x (BN/WN) = MI m16 x NJ n8 MMA tiles.
+template <int BM_, int BN_, int WM_, int WN_>
+struct Cfg {
+  static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_;
+  static constexpr int MI = BM / WM / 16, NJ = BN / WN / 8;
+  static constexpr int LDA_N = BM + 2;  // sA[k][m]  (op(A) = A)
+  static constexpr int LDB_T = BN + 2;  // sB[k][n]  (op(B) = B^T)
+  static_assert(WM * WN * 32 == NT, "8 warps");
+  __host__ __device__ static constexpr int a_elems(bool ta) { return ta ? BM * LDA_T : BK * LDA_N; }
+  __host__ __device__ static constexpr int b_elems(bool tb) { return tb ? BK * LDB_T : BN * LDB_N; }
+  static constexpr int smem(bool ta, bool tb) { return STAGES * (a_elems(ta) + b_elems(tb)) * 8; }
+};
+using CfgBig = Cfg<128, 128, 2, 4>;   // general
+using CfgSkinnyM = Cfg<32, 128, 1, 8>;  // M <= 32 (V^T W products of the QR updates)
+using CfgSkinnyN = Cfg<128, 64, 4, 2>;  // N <= 64 (TRSM leaves, narrow updates)
 
 struct KParams {
   GemmArgs g;
@@ -48,12 +49,15 @@ struct KParams {
   int64_t ldp;
 };
 
-template <bool TA, bool TB, bool V16>
+template <class C, bool TA, bool TB, bool V16>
 __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
+  constexpr int BM = C::BM, BN = C::BN, MI = C::MI, NJ = C::NJ;
+  constexpr int LDA_N = C::LDA_N, LDB_T = C::LDB_T;
+  constexpr int AE = C::a_elems(TA), BE = C::b_elems(TB);
   extern __shared__ __align__(16) double smem[];
   const GemmArgs& p = kp.g;
   double* sAb = smem;
-  double* sBb = smem + STAGES * a_elems<TA>();
+  double* sBb = smem + STAGES * AE;
 
   const int bz = blockIdx.z;
   const int split = blockIdx.y;
@@ -79,7 +83,7 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
   const int M = p.M, N = p.N;
 
   int kb = 0, ke = p.K;
-  if (p.kfrom_n) kb = min(n0, ke);
+  if (p.kfrom_n) kb = min(n0 / BK * BK, ke);
   if (kp.splitk > 1) {
     const int span = ke - kb;
     int len = (span + kp.splitk - 1) / kp.splitk;
@@ -94,59 +98,58 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
   const int64_t lda = p.lda, ldb = p.ldb;
   const int tid = threadIdx.x;
 
-  // Each thread moves four 16-byte chunks (two FP64 values along the contiguous
-  // dimension) per operand per stage.  V16: one 16-byte cp.async with zero
-  // fill; otherwise (odd leading dimension / unaligned base) two 8-byte copies.
-  auto chunk = [&](double* dst, const double* base, int64_t off0, bool in0, bool in1, int64_t step) {
+  // 16-byte chunks (two FP64 values along the contiguous dimension).  V16: one
+  // cp.async of 16 bytes with zero fill; otherwise two 8-byte copies.
+  auto chunk = [&](double* dst, const double* base, int64_t off0, bool in0, bool in1) {
     if (V16) {
       const int bytes = in0 ? (in1 ? 16 : 8) : 0;
       cp_async16(dst, bytes ? base + off0 : base, bytes);
     } else {
       cp_async8(dst, in0 ? base + off0 : base, in0 ? 8 : 0);
-      cp_async8(dst + 1, in1 ? base + off0 + step : base, in1 ? 8 : 0);
+      cp_async8(dst + 1, in1 ? base + off0 + 1 : base, in1 ? 8 : 0);
     }
   };
   auto load_stage = [&](int stage, int k0) {
-    double* sa = sAb + stage * a_elems<TA>();
-    double* sb = sBb + stage * b_elems<TB>();
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int c = tid + i * NT;
+    double* sa = sAb + stage * AE;
+    double* sb = sBb + stage * BE;
+    for (int c = tid; c < BM * BK / 2; c += NT) {
       if (!TA) {
-        const int k = c >> 6, m = (c & 63) * 2;
+        const int k = c / (BM / 2), m = (c % (BM / 2)) * 2;
         const int gm = m0 + m, gk = k0 + k;
         const bool kin = gk < ke;
-        chunk(sa + k * LDA_N + m, A, gm + static_cast<int64_t>(gk) * lda, kin && gm < M, kin && gm + 1 < M, 1);
+        chunk(sa + k * LDA_N + m, A, gm + static_cast<int64_t>(gk) * lda, kin && gm < M, kin && gm + 1 < M);
       } else {
-        const int m = c >> 3, k = (c & 7) * 2;
+        const int m = c / (BK / 2), k = (c % (BK / 2)) * 2;
         const int gm = m0 + m, gk = k0 + k;
-        const bool min_ = gm < M;
-        chunk(sa + m * LDA_T + k, A, gk + static_cast<int64_t>(gm) * lda, min_ && gk < ke, min_ && gk + 1 < ke, 1);
+        const bool mi = gm < M;
+        chunk(sa + m * LDA_T + k, A, gk + static_cast<int64_t>(gm) * lda, mi && gk < ke, mi && gk + 1 < ke);
       }
+    }
+    for (int c = tid; c < BN * BK / 2; c += NT) {
       if (!TB) {
-        const int n = c >> 3, k = (c & 7) * 2;
+        const int n = c / (BK / 2), k = (c % (BK / 2)) * 2;
         const int gn = n0 + n, gk = k0 + k;
-        const bool nin = gn < N;
-        chunk(sb + n * LDB_N + k, B, gk + static_cast<int64_t>(gn) * ldb, nin && gk < ke, nin && gk + 1 < ke, 1);
+        const bool ni = gn < N;
+        chunk(sb + n * LDB_N + k, B, gk + static_cast<int64_t>(gn) * ldb, ni && gk < ke, ni && gk + 1 < ke);
       } else {
-        const int k = c >> 6, n = (c & 63) * 2;
+        const int k = c / (BN / 2), n = (c % (BN / 2)) * 2;
         const int gn = n0 + n, gk = k0 + k;
         const bool kin = gk < ke;
-        chunk(sb + k * LDB_T + n, B, gn + static_cast<int64_t>(gk) * ldb, kin && gn < N, kin && gn + 1 < N, 1);
+        chunk(sb + k * LDB_T + n, B, gn + static_cast<int64_t>(gk) * ldb, kin && gn < N, kin && gn + 1 < N);
       }
     }
   };
 
   const int warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
-  const int wm = (warp & 1) * 64;
-  const int wn = (warp >> 1) * 32;
+  const int wm = (warp % C::WM) * (BM / C::WM);
+  const int wn = (warp / C::WM) * (BN / C::WN);
 
-  double acc[4][4][4];
+  double acc[MI][NJ][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
@@ -165,14 +168,14 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
       if (nk < ktiles) load_stage(nk % STAGES, kb + nk * BK);
       cp_async_commit();
     }
-    const double* sa = sAb + (kt % STAGES) * a_elems<TA>();
-    const double* sb = sBb + (kt % STAGES) * b_elems<TB>();
+    const double* sa = sAb + (kt % STAGES) * AE;
+    const double* sb = sBb + (kt % STAGES) * BE;
 #pragma unroll
     for (int kk = 0; kk < BK / 8; ++kk) {
-      double af[4][4];
-      double bf[4][2];
+      double af[MI][4];
+      double bf[NJ][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < MI; ++i) {
         const int m = wm + i * 16 + 2 * g;
         if (!TA) {
           const double2 v0 = *reinterpret_cast<const double2*>(sa + (kk * 8 + 2 * t) * LDA_N + m);
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
         }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < NJ; ++j) {
         const int n = wn + j * 8 + g;
         if (!TB) {
           const double2 v = *reinterpret_cast<const double2*>(sb + n * LDB_N + kk * 8 + 2 * t);
@@ -203,9 +206,9 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
         }
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+        for (int j = 0; j < NJ; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
     }
   }
   cp_async_wait<0>();
@@ -214,9 +217,9 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
   if (kp.splitk > 1) {
     double* P = kp.P + (static_cast<int64_t>(split) * p.batch + bz) * kp.ldp * N;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < NJ; ++j) {
         const int r = m0 + wm + i * 16 + 2 * g;
         const int c = n0 + wn + j * 8 + 2 * t;
 #pragma unroll
@@ -230,21 +233,21 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
       }
     return;
   }
-  double* C = p.C + static_cast<int64_t>(bz) * p.strideC;
+  double* C_ = p.C + static_cast<int64_t>(bz) * p.strideC;
   const int64_t ldc = p.ldc;
   const double alpha = p.alpha * (p.alpha_vec ? p.alpha_vec[bz] : 1.0);
   const double beta = p.beta;
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < NJ; ++j) {
       const int r = m0 + wm + i * 16 + 2 * g;
       const int c = n0 + wn + j * 8 + 2 * t;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int cc = c + h;
         if (cc >= N || r >= M) continue;
-        double* dst = C + r + static_cast<int64_t>(cc) * ldc;
+        double* dst = C_ + r + static_cast<int64_t>(cc) * ldc;
         double v0 = alpha * acc[i][j][h];
         double v1 = alpha * acc[i][j][2 + h];
         const bool ok0 = !p.tri || r >= cc;
@@ -284,30 +287,54 @@ __global__ void splitk_reduce_kernel(GemmArgs p, int splitk, const double* P, in
   }
 }
 
-template <bool TA, bool TB, bool V16>
+template <class C, bool TA, bool TB, bool V16>
 cudaError_t launch_t(const KParams& kp, dim3 grid, cudaStream_t st) {
-  static bool attr_set = false;
-  constexpr int sm = smem_bytes<TA, TB>();
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<TA, TB, V16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  dgemm_kernel<TA, TB, V16><<<grid, NT, sm, st>>>(kp);
+  static cudaError_t attr = cudaFuncSetAttribute(dgemm_kernel<C, TA, TB, V16>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, C::smem(TA, TB));
+  if (attr != cudaSuccess) return attr;
+  dgemm_kernel<C, TA, TB, V16><<<grid, NT, C::smem(TA, TB), st>>>(kp);
   return cudaGetLastError();
 }
 
-template <bool V16>
+template <class C, bool V16>
 cudaError_t launch_v(const KParams& kp, dim3 grid, cudaStream_t st) {
   const GemmArgs& a = kp.g;
-  if (!a.transA && !a.transB) return launch_t<false, false, V16>(kp, grid, st);
-  if (!a.transA && a.transB) return launch_t<false, true, V16>(kp, grid, st);
-  if (a.transA && !a.transB) return launch_t<true, false, V16>(kp, grid, st);
-  return launch_t<true, true, V16>(kp, grid, st);
+  if (!a.transA && !a.transB) return launch_t<C, false, false, V16>(kp, grid, st);
+  if (!a.transA && a.transB) return launch_t<C, false, true, V16>(kp, grid, st);
+  if (a.transA && !a.transB) return launch_t<C, true, false, V16>(kp, grid, st);
+  return launch_t<C, true, true, V16>(kp, grid, st);
+}
+
+template <class C>
+cudaError_t launch_c(const KParams& kp, dim3 grid, bool v16, cudaStream_t st) {
+  return v16 ? launch_v<C, true>(kp, grid, st) : launch_v<C, false>(kp, grid, st);
+}
+
+// tile shape: 0 = 128x128, 1 = 32x128 (M <= 32), 2 = 128x64 (N <= 64)
+int pick_cfg(const GemmArgs& a) {
+  if (a.tri) return 0;
+  if (a.M <= 32) return 1;
+  if (a.N <= 64) return 2;
+  return 0;
+}
+
+void tile_dims(int cfg, int* bm, int* bn) {
+  if (cfg == 1) {
+    *bm = CfgSkinnyM::BM;
+    *bn = CfgSkinnyM::BN;
+  } else if (cfg == 2) {
+    *bm = CfgSkinnyN::BM;
+    *bn = CfgSkinnyN::BN;
+  } else {
+    *bm = CfgBig::BM;
+    *bn = CfgBig::BN;
+  }
 }
 
 int choose_splitk(const GemmArgs& a, int sms) {
   if (a.splitk >= 1) return a.splitk;
+  int BM, BN;
+  tile_dims(pick_cfg(a), &BM, &BN);
   const int tm = (a.M + BM - 1) / BM, tn = (a.N + BN - 1) / BN;
   const int64_t tiles = a.tri ? static_cast<int64_t>(tm) * (tm + 1) / 2 : static_cast<int64_t>(tm) * tn;
   const int64_t ctas = tiles * a.batch;
@@ -357,6 +384,9 @@ cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
   }
   KParams kp;
   kp.g = a;
+  const int cfg = pick_cfg(a);
+  int BM, BN;
+  tile_dims(cfg, &BM, &BN);
   kp.tiles_m = (a.M + BM - 1) / BM;
   kp.tiles_n = (a.N + BN - 1) / BN;
   kp.splitk = choose_splitk(a, sms);
@@ -374,7 +404,9 @@ cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
                               : static_cast<int64_t>(kp.tiles_m) * kp.tiles_n;
   if (tiles > 0x7fffffff || a.batch > 65535) return cudaErrorInvalidValue;
   dim3 grid(static_cast<unsigned>(tiles), kp.splitk, a.batch);
-  const cudaError_t e = v16 ? launch_v<true>(kp, grid, st) : launch_v<false>(kp, grid, st);
+  const cudaError_t e = cfg == 1 ? launch_c<CfgSkinnyM>(kp, grid, v16, st)
+                        : cfg == 2 ? launch_c<CfgSkinnyN>(kp, grid, v16, st)
+                                   : launch_c<CfgBig>(kp, grid, v16, st);
   if (e != cudaSuccess || kp.splitk <= 1) return e;
   const int64_t total = static_cast<int64_t>(a.M) * a.N;
   int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 4 * sms));

@@ -72,12 +72,15 @@ cudaError_t add_diag(int n, double* A, int64_t lda, double d, cudaStream_t st);
 cudaError_t reduce_sum(const double* partial, int count, double* out, cudaStream_t st);
 
 // ---- Cholesky / triangular (potrf.cu) ----
-// In-place lower Cholesky of nb x nb blocks (nb <= 64), batched; info recorded in status[b].
+// In-place lower Cholesky of nb x nb blocks (nb <= 64), batched; LAPACK INFO (+info_offset)
+// recorded in info[b]; when Dinv != nullptr the inverse of the factor goes to
+// Dinv + b*strideD (64 x 64, ld 64, zeros above the diagonal).
 cudaError_t potrf_leaf(int nb, double* A, int64_t lda, int64_t strideA, int batch, int* info,
-                       int info_offset, cudaStream_t st);
-// In-place inverse of lower-triangular nb x nb blocks (nb <= 64), batched.
-cudaError_t trtri_leaf(int nb, const double* L, int64_t ldl, int64_t strideL, double* Linv,
-                       int64_t ldi, int64_t strideI, int batch, cudaStream_t st);
+                       int info_offset, double* Dinv, int64_t strideD, cudaStream_t st);
+// Inverses of all 64 x 64 diagonal blocks of lower-triangular n x n matrices:
+// block kb of batch entry b -> Dinv + (b*nblk + kb)*4096, nblk = ceil(n/64).
+cudaError_t trtri_blocks(int n, const double* L, int64_t ldl, int64_t strideL, double* Dinv, int batch,
+                         cudaStream_t st);
 
 // ---- Householder QR panel (qr.cu) ----
 // Factor the m x w panel of each batch entry (w <= 32) in place: V below the

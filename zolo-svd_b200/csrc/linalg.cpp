@@ -3,13 +3,12 @@
 #include "linalg.h"
 
 #include <algorithm>
-#include <stdexcept>
 
 namespace zolo {
 
 namespace {
-constexpr int NB = 64;  // leaf of the Cholesky / TRSM recursion
-constexpr int PW = 32;  // Householder panel width
+constexpr int NB = kLeaf;  // leaf of the Cholesky / TRSM recursion
+constexpr int PW = 32;     // Householder panel width
 
 int split_point(int n) {
   int n1 = ((n / 2) + NB - 1) / NB * NB;
@@ -20,7 +19,7 @@ int split_point(int n) {
 }  // namespace
 
 void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
-          int batch, const double* alpha_vec, int tri, int kfrom_n) {
+          int batch, const double* alpha_vec, int tri, int kfrom_n, cudaStream_t st) {
   GemmArgs a;
   a.M = M;
   a.N = N;
@@ -44,57 +43,72 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   a.kfrom_n = kfrom_n;
   const size_t need = dgemm_splitk_bytes(a, num_sms());
   if (need) c.ensure_splitk(need);
-  ck(dgemm(a, c.splitk(), c.stream()));
+  cudaStream_t s = st ? st : c.stream();
+  Profiler::Rec rec;
+  if (c.prof.on) c.prof.begin(0, (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K * batch, s, &rec);
+  ck(dgemm(a, c.splitk(), s));
+  if (c.prof.on) c.prof.end(rec, s);
   c.stats.launches += need ? 2 : 1;
 }
 
-static void potrf_rec(Context& c, int n, Mat A, int batch, int* dinfo, int off) {
+static void potrf_rec(Context& c, int n, Mat A, int batch, int* dinfo, int off, DiagInv D) {
   if (n <= NB) {
-    ck(potrf_leaf(n, A.p, A.ld, A.stride, batch, dinfo, off, c.stream()));
+    Profiler::Rec rec;
+    if (c.prof.on) c.prof.begin(2, static_cast<double>(n) * n * n / 3.0 * batch, c.stream(), &rec);
+    ck(potrf_leaf(n, A.p, A.ld, A.stride, batch, dinfo, off, D.block(off / NB), D.stride, c.stream()));
+    if (c.prof.on) c.prof.end(rec, c.stream());
     c.stats.launches++;
     return;
   }
   const int n1 = split_point(n), n2 = n - n1;
-  potrf_rec(c, n1, A, batch, dinfo, off);
-  // A21 <- A21 L11^{-T}
+  potrf_rec(c, n1, A, batch, dinfo, off, D);
+  // A21 <- A21 L11^{-T}  (out of place through a scratch copy)
   const int64_t ldt = (n2 + 1) / 2 * 2;
   Mat tmp{c.buf("potrf_tmp", static_cast<size_t>(ldt) * n1 * batch), ldt, ldt * n1};
   ck(scale_copy(n2, n1, 1.0, A.at(n1, 0).p, A.ld, A.stride, tmp.p, tmp.ld, tmp.stride, batch, 0.0, c.stream()));
   c.stats.launches++;
-  trsm_rlt(c, n2, n1, A, tmp, A.at(n1, 0), batch);
+  trsm_rlt(c, n2, n1, A, tmp, A.at(n1, 0), batch, D, off / NB);
   // A22 -= A21 A21^T (lower)
   gemm(c, 0, 1, n2, n2, n1, -1.0, A.at(n1, 0), A.at(n1, 0), 1.0, A.at(n1, n1), batch, nullptr, 1, 0);
-  potrf_rec(c, n2, A.at(n1, n1), batch, dinfo, off + n1);
+  potrf_rec(c, n2, A.at(n1, n1), batch, dinfo, off + n1, D);
 }
 
-void potrf(Context& c, int n, Mat A, int batch, int* dinfo) { potrf_rec(c, n, A, batch, dinfo, 0); }
+void potrf(Context& c, int n, Mat A, int batch, int* dinfo, DiagInv D) {
+  // size the scratch of the largest recursion level first (no growth mid-recursion)
+  if (n > NB) {
+    const int n1 = split_point(n), n2 = n - n1;
+    c.buf("potrf_tmp", static_cast<size_t>((n2 + 1) / 2 * 2) * n1 * batch);
+  }
+  potrf_rec(c, n, A, batch, dinfo, 0, D);
+}
 
-void trsm_rlt(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch) {
+void diag_inverses(Context& c, int n, Mat L, int batch, DiagInv D) {
+  ck(trtri_blocks(n, L.p, L.ld, L.stride, D.p, batch, c.stream()));
+  c.stats.launches++;
+}
+
+void trsm_rlt(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv D, int k0) {
   if (n <= NB) {
-    Mat li{c.buf("trsm_linv", static_cast<size_t>(NB) * NB * batch), NB, NB * NB};
-    ck(trtri_leaf(n, L.p, L.ld, L.stride, li.p, li.ld, li.stride, batch, c.stream()));
-    c.stats.launches++;
+    Mat li{D.block(k0), NB, D.stride};
     gemm(c, 0, 1, m, n, n, 1.0, X, li, 0.0, Y, batch);
     return;
   }
   const int n1 = split_point(n), n2 = n - n1;
-  trsm_rlt(c, m, n1, L, X, Y, batch);
+  trsm_rlt(c, m, n1, L, X, Y, batch, D, k0);
   gemm(c, 0, 1, m, n2, n1, -1.0, Y, L.at(n1, 0), 1.0, X.at(0, n1), batch);
-  trsm_rlt(c, m, n2, L.at(n1, n1), X.at(0, n1), Y.at(0, n1), batch);
+  trsm_rlt(c, m, n2, L.at(n1, n1), X.at(0, n1), Y.at(0, n1), batch, D, k0 + n1 / NB);
 }
 
-void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch) {
+void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv D, int k0) {
   if (n <= NB) {
-    Mat li{c.buf("trsm_linv", static_cast<size_t>(NB) * NB * batch), NB, NB * NB};
-    ck(trtri_leaf(n, L.p, L.ld, L.stride, li.p, li.ld, li.stride, batch, c.stream()));
-    c.stats.launches++;
+    Mat li{D.block(k0), NB, D.stride};
     gemm(c, 0, 0, m, n, n, 1.0, X, li, 0.0, Y, batch);
     return;
   }
   const int n1 = split_point(n), n2 = n - n1;
-  trsm_rln(c, m, n2, L.at(n1, n1), X.at(0, n1), Y.at(0, n1), batch);
+  trsm_rln(c, m, n2, L.at(n1, n1), X.at(0, n1), Y.at(0, n1), batch, D, k0 + n1 / NB);
   gemm(c, 0, 0, m, n1, n2, -1.0, Y.at(0, n1), L.at(n1, 0), 1.0, X, batch);
-  trsm_rln(c, m, n1, L, X, Y, batch);
+  trsm_rln(c, m, n1, L, X, Y, batch, D, k0);
 }
 
 static inline int row_hi(int mtot, int m_top, int j, int jb) {
@@ -104,22 +118,48 @@ static inline int row_hi(int mtot, int m_top, int j, int jb) {
 void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch) {
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
-  Mat V{c.buf("qr_v", static_cast<size_t>(ldv) * PW * batch), ldv, ldv * PW};
+  // explicit V of consecutive panels alternates between two buffers (look-ahead)
+  double* vb = c.buf("qr_v2", static_cast<size_t>(ldv) * PW * batch * 2);
+  Mat V[2] = {Mat{vb, ldv, ldv * PW}, Mat{vb + ldv * PW * batch, ldv, ldv * PW}};
   Mat P{c.buf("qr_p", static_cast<size_t>(PW) * n * batch), PW, static_cast<int64_t>(PW) * n};
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
-  for (int j = 0; j < n; j += PW) {
+  cudaStream_t ms = c.stream(), ss = c.side_stream();
+  auto panel = [&](int pj, cudaStream_t st) {
+    const int j = pj * PW;
     const int jb = std::min(PW, n - j);
-    const int rhi = row_hi(mtot, m_top, j, jb);
-    const int mp = rhi - j;
-    ck(qr_panel(mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + (j / PW) * PW * PW, strideT, V.p, V.ld,
-                V.stride, batch, c.stream()));
+    const int mp = row_hi(mtot, m_top, j, jb) - j;
+    Profiler::Rec rec;
+    if (c.prof.on) c.prof.begin(1, 2.0 * mp * static_cast<double>(jb) * jb * batch, st, &rec);
+    ck(qr_panel(mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + pj * PW * PW, strideT, V[pj & 1].p,
+                V[pj & 1].ld, V[pj & 1].stride, batch, st));
+    if (c.prof.on) c.prof.end(rec, st);
     c.stats.launches++;
+  };
+  panel(0, ms);
+  for (int pj = 0; pj < npan; ++pj) {
+    const int j = pj * PW;
+    const int jb = std::min(PW, n - j);
+    const int mp = row_hi(mtot, m_top, j, jb) - j;
     const int nc = n - j - jb;
-    if (nc > 0) {
-      gemm(c, 1, 0, jb, nc, mp, 1.0, V, W.at(j, j + jb), 0.0, P, batch);
-      ck(apply_t(jb, nc, T + (j / PW) * PW * PW, strideT, P.p, P.ld, P.stride, 1, batch, c.stream()));
-      c.stats.launches++;
-      gemm(c, 0, 0, mp, nc, jb, -1.0, V, P, 1.0, W.at(j, j + jb), batch);
+    if (nc <= 0) break;
+    const Mat& Vj = V[pj & 1];
+    // P = T^T V^T W_trail
+    gemm(c, 1, 0, jb, nc, mp, 1.0, Vj, W.at(j, j + jb), 0.0, P, batch);
+    ck(apply_t(jb, nc, T + pj * PW * PW, strideT, P.p, P.ld, P.stride, 1, batch, ms));
+    c.stats.launches++;
+    // next panel's columns first, then the panel on the side stream overlaps the rest
+    const int jb2 = std::min(PW, nc);
+    gemm(c, 0, 0, mp, jb2, jb, -1.0, Vj, P, 1.0, W.at(j, j + jb), batch);
+    const bool overlap = nc > jb2;
+    if (overlap) {
+      ck(cudaEventRecord(c.event(0), ms));
+      ck(cudaStreamWaitEvent(ss, c.event(0), 0));
+      panel(pj + 1, ss);
+      ck(cudaEventRecord(c.event(1), ss));
+      gemm(c, 0, 0, mp, nc - jb2, jb, -1.0, Vj, P.at(0, jb2), 1.0, W.at(j, j + jb + jb2), batch);
+      ck(cudaStreamWaitEvent(ms, c.event(1), 0));
+    } else {
+      panel(pj + 1, ms);
     }
   }
 }
@@ -127,7 +167,7 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
 void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch) {
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
-  Mat V{c.buf("qr_v", static_cast<size_t>(ldv) * PW * batch), ldv, ldv * PW};
+  Mat V{c.buf("qr_v2", static_cast<size_t>(ldv) * PW * batch * 2), ldv, ldv * PW};
   Mat P{c.buf("qr_p", static_cast<size_t>(PW) * n * batch), PW, static_cast<int64_t>(PW) * n};
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
   ck(set_identity(mtot, n, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
@@ -135,8 +175,7 @@ void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q
   for (int pj = npan - 1; pj >= 0; --pj) {
     const int j = pj * PW;
     const int jb = std::min(PW, n - j);
-    const int rhi = row_hi(mtot, m_top, j, jb);
-    const int mp = rhi - j;
+    const int mp = row_hi(mtot, m_top, j, jb) - j;
     const int nc = n - j;
     ck(extract_v(mp, jb, W.at(j, j).p, W.ld, W.stride, V.p, V.ld, V.stride, batch, c.stream()));
     c.stats.launches++;

@@ -15,20 +15,37 @@ struct Mat {
   Mat at(int i, int j) const { return Mat{p + i + static_cast<int64_t>(j) * ld, ld, stride}; }
 };
 
+// Inverses of the 64 x 64 diagonal blocks of a lower-triangular factor:
+// block k of batch entry b at p + b*stride + k*4096 (ld 64).
+struct DiagInv {
+  double* p;
+  int64_t stride;
+  double* block(int k) const { return p + static_cast<int64_t>(k) * 4096; }
+};
+
+constexpr int kLeaf = 64;
+inline int nblocks(int n) { return (n + kLeaf - 1) / kLeaf; }
+
 void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
-          int batch, const double* alpha_vec = nullptr, int tri = 0, int kfrom_n = 0);
+          int batch, const double* alpha_vec = nullptr, int tri = 0, int kfrom_n = 0,
+          cudaStream_t st = nullptr);
 
 // Lower Cholesky in place (n x n), recursive; info[b] > 0 on failure (LAPACK convention).
-void potrf(Context& c, int n, Mat A, int batch, int* dinfo);
-// X(m x n) <- X L^{-T}   (out of place: X is destroyed, result in Y)
-void trsm_rlt(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch);
-// X(m x n) <- X L^{-1}   (out of place: X is destroyed, result in Y)
-void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch);
+// Dinv receives the inverses of the diagonal blocks of L (used by the solves below).
+void potrf(Context& c, int n, Mat A, int batch, int* dinfo, DiagInv Dinv);
+// Dinv for a lower-triangular L that did not come from potrf.
+void diag_inverses(Context& c, int n, Mat L, int batch, DiagInv Dinv);
+// Y = X L^{-T}  (X m x n is destroyed; L's diagonal block k has inverse Dinv.block(k0 + k))
+void trsm_rlt(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv Dinv, int k0 = 0);
+// Y = X L^{-1}
+void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv Dinv, int k0 = 0);
 
 // Householder QR (in place, panels of 32) of the mtot x n matrices W.  With
-// `m_top` >= 0 the matrix is the stack [X (m_top x n); D] where D is upper
+// `m_top` >= 0 the matrix is the stack [X (m_top rows); D] where D is upper
 // triangular: panel j only touches rows j .. m_top + j + 31 (mpdgeqrf.f).
 // tau: n per batch entry; T: ceil(n/32) * 32 * 32 per batch entry.
+// The next panel is factored on a high-priority side stream while the rest of
+// the trailing matrix is updated (look-ahead of depth 1).
 void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch);
 // Explicit Q (mtot x n) from the reflectors of geqrf (mpdorgqr.f / dorgqr).
 void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch);

@@ -68,15 +68,16 @@ void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
 }
 
 // Z(b) = X W_b^{-1} (left = false) or W_b^{-1} X (left = true, square X), W_b = L_b L_b^T.
-void spd_solve(Context& c, int m, int n, const double* X, int64_t ldx, Mat Lw, Mat Z, int batch, bool left) {
+void spd_solve(Context& c, int m, int n, const double* X, int64_t ldx, Mat Lw, DiagInv D, Mat Z, int batch,
+               bool left) {
   const int64_t ldm = even(m);
   Mat Xc{c.buf("Xc", static_cast<size_t>(ldm) * n * batch), ldm, ldm * n};
   Mat Y{c.buf("Y", static_cast<size_t>(ldm) * n * batch), ldm, ldm * n};
   if (!left) {
     ck(scale_copy(m, n, 1.0, X, ldx, 0, Xc.p, Xc.ld, Xc.stride, batch, 0.0, c.stream()));
     c.stats.launches++;
-    trsm_rlt(c, m, n, Lw, Xc, Y, batch);
-    trsm_rln(c, m, n, Lw, Y, Z, batch);
+    trsm_rlt(c, m, n, Lw, Xc, Y, batch, D);
+    trsm_rln(c, m, n, Lw, Y, Z, batch, D);
     return;
   }
   // W^{-1} X = (X^T W^{-1})^T : transpose in, right solves, transpose out
@@ -84,8 +85,8 @@ void spd_solve(Context& c, int m, int n, const double* X, int64_t ldx, Mat Lw, M
     ck(transpose(m, n, X, ldx, Xc.p + b * Xc.stride, Xc.ld, c.stream()));
     c.stats.launches++;
   }
-  trsm_rlt(c, n, m, Lw, Xc, Y, batch);
-  trsm_rln(c, n, m, Lw, Y, Xc, batch);
+  trsm_rlt(c, n, m, Lw, Xc, Y, batch, D);
+  trsm_rln(c, n, m, Lw, Y, Xc, batch, D);
   for (int b = 0; b < batch; ++b) {
     ck(transpose(n, m, Xc.p + b * Xc.stride, Xc.ld, Z.p + b * Z.stride, Z.ld, c.stream()));
     c.stats.launches++;
@@ -140,7 +141,9 @@ int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda
   ck(transpose(n, n, X, ldx, Lt, ldn, c.stream()));
   ck(set_identity(n, n, I, ldn, 0, 1, 1.0, c.stream()));
   c.stats.launches += 2;
-  trsm_rlt(c, n, n, Mat{Lt, ldn, 0}, Mat{I, ldn, 0}, Mat{Ri, ldn, 0}, 1);
+  DiagInv D{c.buf("bnd_dinv", static_cast<size_t>(nblocks(n)) * 4096), 0};
+  diag_inverses(c, n, Mat{Lt, ldn, 0}, 1, D);
+  trsm_rlt(c, n, n, Mat{Lt, ldn, 0}, Mat{I, ldn, 0}, Mat{Ri, ldn, 0}, 1, D);
   double* colsum = c.buf("bnd_colsum", n);
   ck(norm1(n, n, Ri, ldn, colsum, scal + 2, c.stream()));
   ck(frob2(n, n, Ri, ldn, part, scal + 3, c.stream()));
@@ -193,6 +196,7 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
   Mat Qf{c.buf("Qf", static_cast<size_t>(ldw) * n), ldw, 0};
   Mat Z{c.buf("Z", static_cast<size_t>(ldz) * n), ldz, 0};
   Mat G{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
+  DiagInv Dg{c.buf("dinv", static_cast<size_t>(nblocks(n)) * 4096), 0};
   double* tau = c.buf("tau", n);
   double* T = c.buf("qr_t", static_cast<size_t>(npanels(n)) * 1024);
   int* dinfo = c.dinfo();
@@ -214,14 +218,14 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
       ck(add_diag(n, G.p, G.ld, 1.0, c.stream()));
       ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
       c.stats.launches += 2;
-      potrf(c, n, G, 1, dinfo);
+      potrf(c, n, G, 1, dinfo, Dg);
       const int pinfo = read_info(c, dinfo, 1);
       if (pinfo != 0) {
         // not numerically SPD: redo this step with the QR form (the reference ignores PDPOSV's INFO)
         if (c.stats.info == 0) c.stats.info = pinfo;
         use_qr = true;
       } else {
-        spd_solve(c, m, n, X, ldx, G, Z, 1, left);
+        spd_solve(c, m, n, X, ldx, G, Dg, Z, 1, left);
         akk = ak - bk / ckk;
         bkk = bk / ckk;
         c.stats.chol_iterations++;
@@ -294,6 +298,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   Mat Z{c.buf("Z", static_cast<size_t>(sZ) * rk), ldz, sZ};
   Mat G{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
   Mat Wc{W.p, ldn, ldn * n};  // shifted Gram matrices reuse the QR workspace
+  const int64_t sD = static_cast<int64_t>(nblocks(n)) * 4096;
+  DiagInv Dz{c.buf("dinv", static_cast<size_t>(sD) * rk), sD};
   double* tau = c.buf("tau", static_cast<size_t>(n) * rk);
   double* T = c.buf("qr_t", static_cast<size_t>(npanels(n)) * 1024 * rk);
   double* dvec = c.buf("zolo_vec", 64);
@@ -318,13 +324,13 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk, c.stream()));
       ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * rk, c.stream()));
       c.stats.launches += 2;
-      potrf(c, n, Wc, rk, dinfo);
+      potrf(c, n, Wc, rk, dinfo, Dz);
       const int pinfo = read_info(c, dinfo, rk);
       if (pinfo != 0) {
         if (c.stats.info == 0) c.stats.info = pinfo;
         use_qr = true;  // fall back to the QR form for this step
       } else {
-        spd_solve(c, m, n, X, ldx, Wc, Z, rk, left);
+        spd_solve(c, m, n, X, ldx, Wc, Dz, Z, rk, left);
         for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b];
         c.stats.chol_iterations++;
         if (it < 16) c.stats.branch[it] = 2;

@@ -1,7 +1,8 @@
 // Leaf kernels of the recursive Cholesky / triangular solves (FP64).
-// The recursion itself (host side, linalg.cpp) turns all O(n^3) work into DMMA
-// GEMMs; these kernels factor / invert the nb x nb diagonal blocks (nb <= 64)
-// in shared memory, one CTA per batch entry.
+// The recursion (linalg.cpp) turns all O(n^3) work into DMMA GEMMs; these
+// kernels factor the nb x nb diagonal blocks (nb <= 64) in shared memory and
+// also return each block's inverse, which the triangular solves use at their
+// leaves (so no separate inversion pass is needed).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -11,88 +12,163 @@ namespace {
 
 constexpr int LEAF = 64;
 constexpr int LDS = LEAF + 1;
+constexpr int PT = 256;
+constexpr int MAXE = (LEAF * (LEAF + 1) / 2 + PT - 1) / PT;  // lower-triangle elements per thread
 
-__global__ void __launch_bounds__(256) potrf_leaf_kernel(int nb, double* A, int64_t lda, int64_t strideA,
-                                                         int* info, int info_offset) {
-  __shared__ double a[LEAF * LDS];
-  __shared__ int bad;
+// x = l^{-1} for lower-triangular l (nb x nb in shared memory, ld LDS).
+// Column j of the inverse is owned by a group of 4 lanes that split every
+// dot product 4 ways; columns are independent, so only warp-level
+// synchronisation is needed.
+__device__ void tri_inverse_smem(int nb, const double* l, double* x) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = warp * 8 + (lane >> 2);
+  const int q = lane & 3;
+  const bool own = j < nb;
+  if (own) {
+    for (int i = q; i < nb; i += 4) x[i + j * LDS] = 0.0;
+  }
+  __syncwarp();
+  if (own && q == 0) x[j + j * LDS] = 1.0 / l[j + j * LDS];
+  __syncwarp();
+  for (int i = 1; i < nb; ++i) {
+    const bool act = own && i > j;
+    double s = 0.0;
+    if (act)
+      for (int k = j + q; k < i; k += 4) s += l[i + k * LDS] * x[k + j * LDS];
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (act && q == 0) x[i + j * LDS] = -s / l[i + i * LDS];
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(PT) potrf_leaf_kernel(int nb, double* A, int64_t lda, int64_t strideA, int* info,
+                                                        int info_offset, double* Dinv, int64_t strideD) {
+  extern __shared__ double sm[];
+  double* a = sm;
+  double* x = sm + LEAF * LDS;
   double* Ab = A + blockIdx.x * strideA;
   const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    a[i + j * LDS] = (i >= j) ? Ab[i + j * lda] : 0.0;
-  }
-  if (tid == 0) bad = 0;
-  __syncthreads();
-  for (int k = 0; k < nb; ++k) {
-    if (tid == 0) {
-      const double d = a[k + k * LDS];
-      if (!(d > 0.0)) {  // not positive definite (or NaN): LAPACK's INFO = k+1
-        if (!bad && info) atomicCAS(info + blockIdx.x, 0, info_offset + k + 1);
-        bad = 1;
-        a[k + k * LDS] = 1.0;
-      } else {
-        a[k + k * LDS] = sqrt(d);
+  // this thread's lower-triangle elements (packed column by column)
+  int ei[MAXE], ej[MAXE];
+  const int ne = nb * (nb + 1) / 2;
+#pragma unroll
+  for (int q = 0; q < MAXE; ++q) {
+    int e = tid + q * PT;
+    ei[q] = -1;
+    ej[q] = 0;
+    if (e < ne) {
+      int j = 0;
+      while (e >= nb - j) {
+        e -= nb - j;
+        ++j;
       }
+      ei[q] = j + e;
+      ej[q] = j;
     }
-    __syncthreads();
-    const double piv = a[k + k * LDS];
-    for (int i = k + 1 + tid; i < nb; i += blockDim.x) a[i + k * LDS] /= piv;
-    __syncthreads();
-    const int rem = nb - k - 1;
-    for (int e = tid; e < rem * rem; e += blockDim.x) {
-      const int i = k + 1 + e % rem, j = k + 1 + e / rem;
-      if (i >= j) a[i + j * LDS] -= a[i + k * LDS] * a[j + k * LDS];
-    }
+  }
+#pragma unroll
+  for (int q = 0; q < MAXE; ++q)
+    if (ei[q] >= 0) a[ei[q] + ej[q] * LDS] = Ab[ei[q] + ej[q] * lda];
+  __syncthreads();
+  // right-looking elimination on unscaled columns: one barrier per step
+  for (int k = 0; k < nb; ++k) {
+    const double d = a[k + k * LDS];
+    const double inv = (d > 0.0) ? 1.0 / d : 0.0;
+#pragma unroll
+    for (int q = 0; q < MAXE; ++q)
+      if (ei[q] >= 0 && ej[q] > k) a[ei[q] + ej[q] * LDS] -= a[ei[q] + k * LDS] * a[ej[q] + k * LDS] * inv;
     __syncthreads();
   }
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
+  if (tid == 0 && info) {
+    for (int k = 0; k < nb; ++k)
+      if (!(a[k + k * LDS] > 0.0)) {  // LAPACK INFO = first non-positive pivot
+        atomicCAS(info + blockIdx.x, 0, info_offset + k + 1);
+        break;
+      }
+  }
+  // L(i,j) = a(i,j) / sqrt(d_j), L(j,j) = sqrt(d_j)
+  double lv[MAXE];
+#pragma unroll
+  for (int q = 0; q < MAXE; ++q) {
+    lv[q] = 0.0;
+    if (ei[q] >= 0) {
+      const double dj = a[ej[q] + ej[q] * LDS];
+      const double sj = dj > 0.0 ? sqrt(dj) : 1.0;
+      lv[q] = (ei[q] == ej[q]) ? sj : a[ei[q] + ej[q] * LDS] / sj;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < MAXE; ++q)
+    if (ei[q] >= 0) {
+      a[ei[q] + ej[q] * LDS] = lv[q];
+      Ab[ei[q] + ej[q] * lda] = lv[q];
+    }
+  for (int e = tid; e < nb * nb; e += PT) {
     const int i = e % nb, j = e / nb;
-    if (i >= j) Ab[i + j * lda] = a[i + j * LDS];
+    if (i < j) a[i + j * LDS] = 0.0;
+  }
+  __syncthreads();
+  if (Dinv) {
+    tri_inverse_smem(nb, a, x);
+    __syncthreads();
+    double* Db = Dinv + blockIdx.x * strideD;
+    for (int e = tid; e < nb * nb; e += PT) {
+      const int i = e % nb, j = e / nb;
+      Db[i + j * LEAF] = x[i + j * LDS];
+    }
   }
 }
 
-// Linv = L^{-1} for lower-triangular L (nb <= 64); zeros above the diagonal.
-// Thread j forward-substitutes column j of the inverse directly in global memory.
-__global__ void __launch_bounds__(LEAF) trtri_leaf_kernel(int nb, const double* L, int64_t ldl, int64_t strideL,
-                                                         double* Linv, int64_t ldi, int64_t strideI) {
-  __shared__ double l[LEAF * LDS];
-  const double* Lb = L + blockIdx.x * strideL;
-  double* Ib = Linv + blockIdx.x * strideI;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
+// Inverses of the diagonal blocks of a lower-triangular n x n matrix:
+// block kb (rows/cols kb*64 ..) of batch entry b goes to Dinv + (b*nblk + kb)*64*64.
+__global__ void __launch_bounds__(PT) trtri_blocks_kernel(int n, const double* L, int64_t ldl, int64_t strideL,
+                                                          double* Dinv, int nblk) {
+  extern __shared__ double sm[];
+  double* l = sm;
+  double* x = sm + LEAF * LDS;
+  const int kb = blockIdx.x, b = blockIdx.y;
+  const int o = kb * LEAF;
+  const int nb = min(LEAF, n - o);
+  const double* Lb = L + b * strideL + o + static_cast<int64_t>(o) * ldl;
+  for (int e = threadIdx.x; e < nb * nb; e += PT) {
     const int i = e % nb, j = e / nb;
-    l[i + j * LDS] = (i >= j) ? Lb[i + j * ldl] : 0.0;
+    l[i + j * LDS] = (i >= j) ? Lb[i + static_cast<int64_t>(j) * ldl] : 0.0;
   }
   __syncthreads();
-  const int j = tid;
-  if (j < nb) {
-    double* x = Ib + j * ldi;
-    for (int i = 0; i < j; ++i) x[i] = 0.0;
-    x[j] = 1.0 / l[j + j * LDS];
-    for (int i = j + 1; i < nb; ++i) {
-      double s = 0.0;
-      for (int k = j; k < i; ++k) s += l[i + k * LDS] * x[k];
-      x[i] = -s / l[i + i * LDS];
-    }
+  tri_inverse_smem(nb, l, x);
+  __syncthreads();
+  double* Db = Dinv + (static_cast<int64_t>(b) * nblk + kb) * LEAF * LEAF;
+  for (int e = threadIdx.x; e < nb * nb; e += PT) {
+    const int i = e % nb, j = e / nb;
+    Db[i + j * LEAF] = x[i + j * LDS];
   }
 }
+
+constexpr int SMEM_BYTES = 2 * LEAF * LDS * 8;
 
 }  // namespace
 
 cudaError_t potrf_leaf(int nb, double* A, int64_t lda, int64_t strideA, int batch, int* info, int info_offset,
-                       cudaStream_t st) {
+                       double* Dinv, int64_t strideD, cudaStream_t st) {
   if (nb <= 0 || batch <= 0) return cudaSuccess;
   if (nb > LEAF) return cudaErrorInvalidValue;
-  potrf_leaf_kernel<<<batch, 256, 0, st>>>(nb, A, lda, strideA, info, info_offset);
+  static cudaError_t attr = cudaFuncSetAttribute(potrf_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 SMEM_BYTES);
+  if (attr != cudaSuccess) return attr;
+  potrf_leaf_kernel<<<batch, PT, SMEM_BYTES, st>>>(nb, A, lda, strideA, info, info_offset, Dinv, strideD);
   return cudaGetLastError();
 }
 
-cudaError_t trtri_leaf(int nb, const double* L, int64_t ldl, int64_t strideL, double* Linv, int64_t ldi,
-                       int64_t strideI, int batch, cudaStream_t st) {
-  if (nb <= 0 || batch <= 0) return cudaSuccess;
-  if (nb > LEAF) return cudaErrorInvalidValue;
-  trtri_leaf_kernel<<<batch, LEAF, 0, st>>>(nb, L, ldl, strideL, Linv, ldi, strideI);
+cudaError_t trtri_blocks(int n, const double* L, int64_t ldl, int64_t strideL, double* Dinv, int batch,
+                         cudaStream_t st) {
+  if (n <= 0 || batch <= 0) return cudaSuccess;
+  static cudaError_t attr = cudaFuncSetAttribute(trtri_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 SMEM_BYTES);
+  if (attr != cudaSuccess) return attr;
+  const int nblk = (n + LEAF - 1) / LEAF;
+  trtri_blocks_kernel<<<dim3(nblk, batch), PT, SMEM_BYTES, st>>>(n, L, ldl, strideL, Dinv, nblk);
   return cudaGetLastError();
 }
 

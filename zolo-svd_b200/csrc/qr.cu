@@ -1,19 +1,19 @@
 // Householder panel factorisation for the blocked QR of the stacked matrix
-// [X; sqrt(c) I] (mpdgeqrf.f:252-313 / PDGEQR2 semantics, LAPACK dlarfg
-// conventions) on one thread-block cluster per panel.
+// [X; sqrt(c) I] (mpdgeqrf.f:252-313 / PDGEQR2 semantics, LAPACK dlarfg and
+// dlarft conventions) on one thread-block cluster per panel.
 //
-// The m x w panel (w <= 32) is split by rows over the CL CTAs of a cluster.
-// Column k costs ONE pass over the CTA's rows and ONE cluster barrier:
-//   * the pass applies reflector k-1 to the remaining columns and, on the
-//     fly, accumulates the partial sums needed by reflector k
-//     (||x_below||^2 and x_below . a_c for every later column c);
-//   * the partials are block-reduced into this CTA's shared memory; after the
-//     barrier every CTA sums all CTAs' partials through distributed shared
-//     memory in the same fixed order, so all CTAs derive bit-identical
-//     beta / tau / w = v^T A and no second barrier is needed (partials are
-//     double-buffered by column parity).
-// After the last column the CTAs reduce V^T V the same way and rank 0 forms
-// the triangular factor T of I - V T V^T (dlarft, forward, columnwise).
+// The m x w panel (w <= 32) is split by rows over the CL CTAs of a cluster;
+// each CTA keeps its rows in shared memory when they fit.  Column k costs ONE
+// pass over the CTA's rows and ONE cluster barrier:
+//   * the pass applies reflector k to the remaining columns and accumulates,
+//     in the same sweep, everything the next step needs: ||x_below||^2 and
+//     x_below . a_c of column k+1, and the Gram column V(:,0:k)^T v_k that
+//     the compact-WY factor T needs;
+//   * the 65 partial sums are block-reduced (warp reduce-scatter) into this
+//     CTA's shared memory; after the barrier every CTA gathers all CTAs'
+//     partials through distributed shared memory and sums them in the same
+//     fixed order, so all CTAs derive bit-identical beta / tau / v^T A and the
+//     same T column; partials are double-buffered by column parity.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -27,13 +27,17 @@ namespace zolo {
 
 namespace {
 
-constexpr int QW = 32;    // max panel width
-constexpr int QT = 256;   // threads per CTA
+constexpr int QW = 32;   // max panel width
+constexpr int QT = 256;  // threads per CTA
 constexpr int NWARP = QT / 32;
-constexpr int SLOT = 1 + QW + QW;  // s0, d[QW], rowk[QW]
+constexpr int SLOT = 1 + 2 * QW;  // s0, d[QW], g[QW]
+constexpr int ROWK = SLOT;        // pivot row of the next column follows the partials
+constexpr int SLOT_ALL = SLOT + QW;
+constexpr int MAX_CL = 16;
+constexpr size_t SMEM_CHUNK_CAP = 190 * 1024;
 
 struct PanelArgs {
-  int m, w, rows_per;
+  int m, w, rows_per, rp_ld;  // rp_ld: leading dimension of the shared-memory chunk
   double* A;
   int64_t lda, strideA;
   double* tau;
@@ -44,33 +48,37 @@ struct PanelArgs {
   int64_t ldv, strideV;
 };
 
-__device__ void block_reduce_vec(double (&acc)[QW + 1], double* red, double* out, int nvals) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// after the call lane l holds in v[0] the warp sum of value index l
+ZDEV void warp_reduce_scatter32(double (&v)[QW], int lane) {
 #pragma unroll
-  for (int c = 0; c < QW + 1; ++c) {
-    if (c < nvals) {
-      double v = warp_sum(acc[c]);
-      if (lane == 0) red[warp * (QW + 1) + c] = v;
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool up = lane & o;
+#pragma unroll
+    for (int i = 0; i < o; ++i) {
+      const double send = up ? v[i] : v[i + o];
+      const double keep = up ? v[i + o] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
     }
   }
-  __syncthreads();
-  if (threadIdx.x < nvals) {
-    double s = 0.0;
-    for (int q = 0; q < NWARP; ++q) s += red[q * (QW + 1) + threadIdx.x];
-    out[threadIdx.x] = s;
-  }
-  __syncthreads();
 }
 
+struct PanelShared {
+  double part[2][SLOT_ALL];
+  double red[NWARP][SLOT];
+  double gat[MAX_CL][SLOT];
+  double sum[SLOT];
+  double rowk[QW];
+  double colk[QW];
+  double tauv[QW];
+  double T[QW * QW];
+};
+
+template <bool SMEM>
 __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
   cg::cluster_group cluster = cg::this_cluster();
-  __shared__ double part[2][SLOT];
-  __shared__ double red[NWARP * (QW + 1)];
-  __shared__ double vtv[QW * QW];
-  __shared__ double colk[QW];  // scratch: wv[c]
-  __shared__ double tvec[QW];
-  __shared__ double gram[QW * QW];
-  __shared__ double vt[32 * (QW + 1)];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PanelShared& S = *reinterpret_cast<PanelShared*>(smem_raw);
+  double* chunk = reinterpret_cast<double*>(smem_raw + ((sizeof(PanelShared) + 15) / 16) * 16);
 
   const int rank = static_cast<int>(cluster.block_rank());
   const int CL = static_cast<int>(cluster.num_blocks());
@@ -81,43 +89,100 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
   const int64_t lda = p.lda, ldv = p.ldv;
   const int r0 = rank * p.rows_per;
   const int r1 = min(m, r0 + p.rows_per);
-  const int tid = threadIdx.x;
+  const int nloc = max(r1 - r0, 0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int rp = p.rp_ld;
 
-  double acc[QW + 1];
+  // element (local row rl of this CTA, column c) of the panel
+  auto at = [&](int rl, int c) -> double& {
+    if (SMEM) return chunk[c * rp + rl];
+    return A[(r0 + rl) + c * lda];
+  };
+
+  if (SMEM) {
+    for (int c = 0; c < w; ++c)
+      for (int rl = tid; rl < nloc; rl += QT) chunk[c * rp + rl] = A[(r0 + rl) + c * lda];
+  }
+  for (int e = tid; e < QW * QW; e += QT) S.T[e] = 0.0;
+
+  double acc_s0;
+  double accd[QW], accg[QW];
+
+  auto reduce_and_publish = [&](double* out) {
+    const double s0w = warp_sum(acc_s0);
+    warp_reduce_scatter32(accd, lane);
+    warp_reduce_scatter32(accg, lane);
+    if (lane == 0) S.red[warp][0] = s0w;
+    S.red[warp][1 + lane] = accd[0];
+    S.red[warp][1 + QW + lane] = accg[0];
+    __syncthreads();
+    if (tid < SLOT) {
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < NWARP; ++q) s += S.red[q][tid];
+      out[tid] = s;
+    }
+  };
 
   // ---- partials for column 0 ----
+  acc_s0 = 0.0;
 #pragma unroll
-  for (int c = 0; c < QW + 1; ++c) acc[c] = 0.0;
-  for (int r = r0 + tid; r < r1; r += QT) {
-    const double x = A[r];
+  for (int c = 0; c < QW; ++c) accd[c] = accg[c] = 0.0;
+  __syncthreads();
+  for (int rl = tid; rl < nloc; rl += QT) {
+    const int r = r0 + rl;
+    const double x = at(rl, 0);
     if (r > 0) {
-      acc[0] += x * x;
+      acc_s0 += x * x;
 #pragma unroll
       for (int c = 1; c < QW; ++c)
-        if (c < w) acc[1 + c] += x * A[r + c * lda];
+        if (c < w) accd[c] += x * at(rl, c);
     } else {
 #pragma unroll
       for (int c = 0; c < QW; ++c)
-        if (c < w) part[0][1 + QW + c] = A[c * lda];
+        if (c < w) S.part[0][ROWK + c] = at(rl, c);
     }
   }
-  block_reduce_vec(acc, red, part[0], 1 + w);
+  reduce_and_publish(S.part[0]);
   cluster.sync();
 
-  for (int k = 0; k < w; ++k) {
+  for (int k = 0; k <= w; ++k) {
     const int buf = k & 1;
-    const int owner = k / p.rows_per;
-    // gather partials (fixed order -> identical on every CTA)
-    double s0 = 0.0;
-    for (int q = 0; q < CL; ++q) s0 += cluster.map_shared_rank(&part[buf][0], q)[0];
-    if (tid < w) {
-      double d = 0.0;
-      for (int q = 0; q < CL; ++q) d += cluster.map_shared_rank(&part[buf][0], q)[1 + tid];
-      colk[tid] = d;  // x_below . a_c
-      tvec[tid] = cluster.map_shared_rank(&part[buf][0], owner)[1 + QW + tid];  // row k
+    // ---- gather the partials of all CTAs (one remote load per element) ----
+    for (int e = tid; e < CL * SLOT; e += QT) {
+      const int q = e / SLOT, i = e - q * SLOT;
+      S.gat[q][i] = cluster.map_shared_rank(&S.part[buf][0], q)[i];
+    }
+    if (k < w) {
+      const int owner = k / p.rows_per;
+      if (tid < w) S.rowk[tid] = cluster.map_shared_rank(&S.part[buf][0], owner)[ROWK + tid];
     }
     __syncthreads();
-    const double alpha = tvec[k];
+    if (tid < SLOT) {
+      double s = 0.0;
+      for (int q = 0; q < CL; ++q) s += S.gat[q][tid];
+      S.sum[tid] = s;
+    }
+    __syncthreads();
+    // ---- T column k-1 from the Gram column g = V(:,0:k-1)^T v_{k-1} (dlarft) ----
+    if (k > 0) {
+      const int kc = k - 1;
+      const double tk = S.tauv[kc];
+      double tv = 0.0;
+      if (tid < kc) {
+        for (int j = tid; j < kc; ++j) tv += S.T[tid + j * QW] * S.sum[1 + QW + j];
+        tv = -tk * tv;
+      }
+      __syncthreads();
+      if (tid < kc) S.T[tid + kc * QW] = tv;
+      if (tid == 0) S.T[kc + kc * QW] = tk;
+      __syncthreads();
+    }
+    if (k == w) break;
+
+    // ---- reflector k (dlarfg) ----
+    const double s0 = S.sum[0];
+    const double alpha = S.rowk[k];
     double beta, tau, scal;
     if (s0 == 0.0) {
       tau = 0.0;
@@ -128,117 +193,77 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
       tau = (beta - alpha) / beta;
       scal = 1.0 / (alpha - beta);
     }
+    if (tid < w) S.colk[tid] = (tid > k) ? S.rowk[tid] + scal * S.sum[1 + tid] : 0.0;  // v^T a_c
+    if (tid == 0) {
+      S.tauv[k] = tau;
+      if (rank == 0) p.tau[b * p.strideTau + k] = tau;
+    }
     __syncthreads();
-    if (tid < w) colk[tid] = (tid > k) ? tvec[tid] + scal * colk[tid] : 0.0;  // w_c = v^T a_c
-    __syncthreads();
-    if (rank == 0 && tid == 0) p.tau[b * p.strideTau + k] = tau;
 
-    // apply reflector k, accumulate partials for column k+1
+    // ---- apply reflector k; accumulate partials of column k+1 and the Gram column of v_k ----
+    acc_s0 = 0.0;
 #pragma unroll
-    for (int c = 0; c < QW + 1; ++c) acc[c] = 0.0;
+    for (int c = 0; c < QW; ++c) accd[c] = accg[c] = 0.0;
     const int nk = k + 1;
-    for (int r = r0 + tid; r < r1; r += QT) {
+    for (int rl = tid; rl < nloc; rl += QT) {
+      const int r = r0 + rl;
       if (r < k) {
         V[r + k * ldv] = 0.0;
         continue;
       }
       if (r == k) {
-        A[r + k * lda] = beta;
+        at(rl, k) = beta;
         V[r + k * ldv] = 1.0;
 #pragma unroll
-        for (int c = 0; c < QW; ++c)
-          if (c > k && c < w) A[r + c * lda] -= tau * colk[c];
+        for (int c = 0; c < QW; ++c) {
+          if (c > k && c < w) at(rl, c) -= tau * S.colk[c];
+          if (c < k) accg[c] += at(rl, c);  // V(k, c) * 1
+        }
+        if (nk < w) {
+#pragma unroll
+          for (int c = 0; c < QW; ++c)
+            if (c >= nk && c < w) S.part[buf ^ 1][ROWK + c] = at(rl, c);
+        }
         continue;
       }
-      const double v = A[r + k * lda] * scal;
-      A[r + k * lda] = v;
+      const double v = at(rl, k) * scal;
+      at(rl, k) = v;
       V[r + k * ldv] = v;
       double xn = 0.0;
 #pragma unroll
       for (int c = 0; c < QW; ++c) {
-        if (c > k && c < w) {
-          const double a = A[r + c * lda] - tau * v * colk[c];
-          A[r + c * lda] = a;
+        if (c < k) {
+          accg[c] += at(rl, c) * v;
+        } else if (c > k && c < w) {
+          const double a = at(rl, c) - tau * v * S.colk[c];
+          at(rl, c) = a;
           if (c == nk) {
             xn = a;
-            if (r > nk) acc[0] += a * a;
+            if (r > nk) acc_s0 += a * a;
           } else if (r > nk) {
-            acc[1 + c] += xn * a;
+            accd[c] += xn * a;
           }
         }
       }
       if (r == nk && nk < w) {
-        // pivot row of the next column: publish its entries
-        double* dst = &part[buf ^ 1][1 + QW];
 #pragma unroll
         for (int c = 0; c < QW; ++c)
-          if (c >= nk && c < w) dst[c] = A[r + c * lda];
+          if (c >= nk && c < w) S.part[buf ^ 1][ROWK + c] = at(rl, c);
       }
     }
-    if (nk < w) block_reduce_vec(acc, red, part[buf ^ 1], 1 + w);
+    reduce_and_publish(S.part[buf ^ 1]);
     cluster.sync();
   }
 
-  // ---- T factor: reduce V^T V, rank 0 runs the dlarft recurrence ----
-  {
-    // partial V^T V over this CTA's rows, staged through shared memory in 32-row tiles
-    double s[(QW * QW + QT - 1) / QT];
-#pragma unroll
-    for (int q = 0; q < (QW * QW + QT - 1) / QT; ++q) s[q] = 0.0;
-    for (int rb = r0; rb < r1; rb += 32) {
-      __syncthreads();
-      for (int e = tid; e < 32 * QW; e += QT) {
-        const int rr = e % 32, c = e / 32;
-        const int r = rb + rr;
-        vt[rr * (QW + 1) + c] = (r < r1 && c < w) ? V[r + c * ldv] : 0.0;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < (QW * QW + QT - 1) / QT; ++q) {
-        const int e = tid + q * QT;
-        const int i = e % QW, j = e / QW;
-        if (i <= j && j < w) {
-          double acc2 = 0.0;
-#pragma unroll 8
-          for (int rr = 0; rr < 32; ++rr) acc2 += vt[rr * (QW + 1) + i] * vt[rr * (QW + 1) + j];
-          s[q] += acc2;
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < (QW * QW + QT - 1) / QT; ++q) vtv[tid + q * QT] = s[q];
+  if (SMEM) {
+    for (int c = 0; c < w; ++c)
+      for (int rl = tid; rl < nloc; rl += QT) A[(r0 + rl) + c * lda] = chunk[c * rp + rl];
   }
-  cluster.sync();
   if (rank == 0) {
-    for (int e = tid; e < w * w; e += QT) {
-      const int i = e % w, j = e / w;
-      double s = 0.0;
-      if (i <= j)
-        for (int q = 0; q < CL; ++q) s += cluster.map_shared_rank(vtv, q)[i + j * QW];
-      gram[i + j * QW] = s;
-    }
-    __syncthreads();
     double* T = p.T + b * p.strideT;
-    const double* tau = p.tau + b * p.strideTau;
-    // T(k,k) = tau_k ; T(0:k,k) = -tau_k * T(0:k,0:k) * gram(0:k,k)
-    for (int k = 0; k < w; ++k) {
-      if (tid < k) {
-        double s = 0.0;
-        for (int j = tid; j < k; ++j) s += T[tid + j * QW] * gram[j + k * QW];
-        tvec[tid] = -tau[k] * s;
-      }
-      __syncthreads();
-      if (tid < QW) {
-        double v;
-        if (tid < k) v = tvec[tid];
-        else if (tid == k) v = tau[k];
-        else v = 0.0;
-        T[tid + k * QW] = v;
-      }
-      __syncthreads();
-    }
+    for (int e = tid; e < QW * QW; e += QT) T[e] = S.T[e];
   }
-  cluster.sync();  // keep every CTA's shared memory alive until rank 0 has read it
+  cluster.sync();  // no CTA leaves while others may still read its shared memory
 }
 
 __global__ void extract_v_kernel(int m, int w, const double* __restrict__ A, int64_t lda, int64_t strideA,
@@ -284,6 +309,65 @@ __global__ void apply_t_kernel(int w, int n, const double* __restrict__ T, int64
   }
 }
 
+constexpr size_t shared_base() { return ((sizeof(PanelShared) + 15) / 16) * 16; }
+
+template <bool SMEM>
+cudaError_t set_attrs() {
+  static cudaError_t done = cudaErrorNotReady;
+  if (done == cudaErrorNotReady) {
+    done = cudaFuncSetAttribute(qr_panel_kernel<SMEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(shared_base() + SMEM_CHUNK_CAP + 64));
+    if (done == cudaSuccess)
+      done = cudaFuncSetAttribute(qr_panel_kernel<SMEM>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  }
+  return done;
+}
+
+template <bool SMEM>
+cudaError_t launch_panel(const PanelArgs& pa, int cl, int batch, size_t smem, cudaStream_t st) {
+  cudaError_t e = set_attrs<SMEM>();
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl, batch, 1);
+  cfg.blockDim = dim3(QT, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr_l[1];
+  attr_l[0].id = cudaLaunchAttributeClusterDimension;
+  attr_l[0].val.clusterDim.x = cl;
+  attr_l[0].val.clusterDim.y = 1;
+  attr_l[0].val.clusterDim.z = 1;
+  cfg.attrs = attr_l;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, qr_panel_kernel<SMEM>, pa);
+}
+
+// 16-CTA clusters are non-portable: use them only if the device can place one
+// with the largest shared-memory footprint; otherwise the portable 8.
+int max_cluster() {
+  static int mc = 0;
+  if (!mc) {
+    mc = 8;
+    if (set_attrs<true>() == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(16, 1, 1);
+      cfg.blockDim = dim3(QT, 1, 1);
+      cfg.dynamicSmemBytes = shared_base() + SMEM_CHUNK_CAP;
+      cudaLaunchAttribute a[1];
+      a[0].id = cudaLaunchAttributeClusterDimension;
+      a[0].val.clusterDim.x = 16;
+      a[0].val.clusterDim.y = 1;
+      a[0].val.clusterDim.z = 1;
+      cfg.attrs = a;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, qr_panel_kernel<true>, &cfg) == cudaSuccess && n > 0) mc = 16;
+    }
+    cudaGetLastError();
+  }
+  return mc;
+}
+
 }  // namespace
 
 cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, double* tau, int64_t strideTau,
@@ -291,12 +375,17 @@ cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, doub
                      cudaStream_t st) {
   if (m <= 0 || w <= 0 || batch <= 0) return cudaSuccess;
   if (w > QW || m < w) return cudaErrorInvalidValue;
-  int cl = (m + 511) / 512;
-  cl = std::max(1, std::min(cl, 8));
+  const int maxcl = max_cluster();
+  // smallest cluster whose per-CTA row chunk fits in shared memory, with at most ~512 rows per CTA
+  int cl = 1;
+  while (cl < maxcl && (static_cast<size_t>(((m + cl - 1) / cl) | 1) * w * 8 > SMEM_CHUNK_CAP ||
+                        (m + cl - 1) / cl > 512))
+    cl *= 2;
   PanelArgs pa;
   pa.m = m;
   pa.w = w;
   pa.rows_per = (m + cl - 1) / cl;
+  pa.rp_ld = pa.rows_per | 1;  // odd stride
   pa.A = A;
   pa.lda = lda;
   pa.strideA = strideA;
@@ -307,19 +396,9 @@ cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, doub
   pa.V = Vexp;
   pa.ldv = ldv;
   pa.strideV = strideV;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(cl, batch, 1);
-  cfg.blockDim = dim3(QT, 1, 1);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = cl;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, qr_panel_kernel, pa);
+  const size_t chunk = static_cast<size_t>(pa.rp_ld) * w * 8;
+  if (chunk <= SMEM_CHUNK_CAP) return launch_panel<true>(pa, cl, batch, shared_base() + chunk, st);
+  return launch_panel<false>(pa, cl, batch, shared_base(), st);
 }
 
 cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t strideA, double* V, int64_t ldv,
