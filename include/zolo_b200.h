@@ -165,6 +165,22 @@ int zolo_zolochol_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t l
 int zolo_formx2_dev(zolo_handle_t h, int m, int n, double fone, double* dX, int64_t ldx, const double* dZ,
                     int64_t ldz, double* err);
 
+/* ---- allocation-free entry point (no counterpart in the reference) ----
+ * Lower Cholesky in place of an n x n SPD matrix on the caller's stream, with no
+ * device allocation and no handle: for callers that cannot let a library call
+ * cudaMalloc -- hosts whose device memory is owned entirely by another allocator
+ * (a framework's caching pool or an application arena) and latency-sensitive hosts
+ * that cannot accept cudaMalloc's device-wide synchronisation.  Same algorithm and
+ * result as zolo_dpotrf_dev.  Its scratch is a fixed 2.5 MiB static device array held
+ * by every GPU that loads the library, so n <= ZOLO_NOALLOC_MAX_N.  The first call on
+ * a device looks the array's address up (cudaGetSymbolAddress) and should be made
+ * before any stream capture.  All calls share the scratch: calls that overlap on the
+ * GPU race and must be serialised by the caller.  Synchronises `stream` before
+ * returning.  Returns LAPACK INFO (> 0: not positive definite), -1 if n < 0 or
+ * n > ZOLO_NOALLOC_MAX_N, -3 if lda < max(1,n), -1000 - cudaError on a CUDA error. */
+#define ZOLO_NOALLOC_MAX_N 1024
+int zolo_dpotrf_noalloc(int n, double* dA, int64_t lda, void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

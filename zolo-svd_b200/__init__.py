@@ -110,6 +110,7 @@ _SIGS = [
                                     C.c_void_p, C.c_int64]),
     ("zolo_formx2_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64, C.c_void_p,
                                   C.c_int64, c_double_p]),
+    ("zolo_dpotrf_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_int64, C.c_void_p]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_"]
