@@ -307,8 +307,13 @@ def run_gpu(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_ms = float(tt.item())
 
-    g = prof["dgemm"]
+    gk = [k for k in prof if k.startswith("dgemm")]
+    g = {"ms": sum(prof[k]["ms"] for k in gk), "flops": sum(prof[k]["flops"] for k in gk),
+         "launches": sum(prof[k]["launches"] for k in gk)}
     achieved = g["flops"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else 0.0
+    per_class = {k: {"launches_per_step": v["launches"] / args.steps, "ms_per_step": v["ms"] / args.steps,
+                     "tflops": (v["flops"] / (v["ms"] * 1e-3) / 1e12) if v["ms"] > 0 else None}
+                 for k, v in prof.items()}
     out = None
     if rank == 0:
         out = {
@@ -326,7 +331,7 @@ def run_gpu(args):
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor)",
                          "traffic": None, "share_of_step": g["ms"] / (t_ms * args.steps) if t_ms else None},
-            "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in prof.items()},
+            "kernel_classes": per_class,
             "e2e": {"value": e2e_ms / 1e3, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n,
                     "d2h_bytes_per_step": 16 * n * n},
             "gpu_launches": int(launches),

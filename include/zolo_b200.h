@@ -66,10 +66,15 @@ int zolo_default_handle(zolo_handle_t* handle);
 int zolo_release_workspace(zolo_handle_t handle);
 const char* zolo_version(void);
 /* Per-kernel-class device timing with CUDA events on the launching streams
- * (class 0 = DMMA GEMM, 1 = Householder panel, 2 = Cholesky leaf).  While enabled,
- * zolo_profile_read returns, per class, {launches, milliseconds, algorithmic flops}
- * accumulated since the last reset (out[3*cls + 0..2]). */
+ * (0 = DMMA GEMM general shapes, 1 = Householder panel, 2 = Cholesky leaf,
+ * 3 = GEMM M <= 32, 4 = GEMM N <= 64, 5 = GEMM rank-k K <= 64, 6 = GEMM lower
+ * triangle).  While enabled, zolo_profile_read fills out[3*cls + 0..2] =
+ * {launches, milliseconds, algorithmic flops} accumulated since the last reset
+ * (out holds 21 doubles). */
 int zolo_profile_enable(zolo_handle_t handle, int on);
+/* Thread-block-cluster size the Householder panel kernel uses for an m x w panel on the
+ * current device (negative when the rows do not fit in shared memory). */
+int zolo_panel_cluster_size(int m, int w);
 int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
 
 /* ---- host scalar routines (no GPU needed) ---- */

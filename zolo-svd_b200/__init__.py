@@ -69,6 +69,7 @@ _SIGS = [
     ("zolo_default_handle", C.c_int, [C.POINTER(C.c_void_p)]),
     ("zolo_release_workspace", C.c_int, [C.c_void_p]),
     ("zolo_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("zolo_panel_cluster_size", C.c_int, [C.c_int, C.c_int]),
     ("zolo_profile_read", C.c_int, [C.c_void_p, c_double_p, C.c_int]),
     ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_mellipke", None, [C.c_double, C.c_double, c_double_p, c_double_p]),
@@ -112,6 +113,8 @@ _SIGS = [
                                   C.c_int64, c_double_p]),
     ("zolo_dpotrf_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_int64, C.c_void_p]),
 ]
+
+PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_"]
 
@@ -289,9 +292,9 @@ class Handle:
 
     def profile_read(self, reset: bool = True) -> dict:
         """Per kernel class: launches, device ms (CUDA events) and algorithmic flops."""
-        out = np.zeros(9)
+        out = np.zeros(3 * len(PROFILE_CLASSES))
         lib().zolo_profile_read(self.ptr, _dp(out), 1 if reset else 0)
-        names = ["dgemm", "qr_panel", "potrf_leaf"]
+        names = PROFILE_CLASSES
         return {nm: dict(launches=int(out[3 * i]), ms=float(out[3 * i + 1]), flops=float(out[3 * i + 2]))
                 for i, nm in enumerate(names)}
 

@@ -27,9 +27,11 @@ struct Stats {
 };
 
 // Optional per-kernel-class timing with CUDA events recorded around launches on
-// their own stream (class 0 = DMMA GEMM, 1 = Householder panel, 2 = Cholesky leaf).
+// their own stream: 0 = DMMA GEMM (general shapes, K > 64), 1 = Householder panel,
+// 2 = Cholesky leaf, 3 = GEMM with M <= 32, 4 = GEMM with N <= 64,
+// 5 = GEMM rank-k update (K <= 64), 6 = GEMM lower-triangle output.
 struct Profiler {
-  static constexpr int kClasses = 3;
+  static constexpr int kClasses = 7;
   bool on = false;
   struct Rec {
     cudaEvent_t a, b;
@@ -38,7 +40,7 @@ struct Profiler {
   };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
-  double launches[kClasses] = {0, 0, 0}, ms[kClasses] = {0, 0, 0}, flops[kClasses] = {0, 0, 0};
+  double launches[kClasses] = {}, ms[kClasses] = {}, flops[kClasses] = {};
   cudaEvent_t take();
   void begin(int cls, double fl, cudaStream_t st, Rec* r);
   void end(Rec& r, cudaStream_t st);

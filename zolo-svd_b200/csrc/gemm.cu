@@ -21,39 +21,41 @@ namespace zolo {
 
 namespace {
 
-constexpr int BK = 16, STAGES = 4, NT = 256;
+constexpr int BK = 16, NT = 256;
 constexpr int LDA_T = BK + 4;  // sA[m][k]  (op(A) = A^T)
 constexpr int LDB_N = BK + 8;  // sB[n][k]  (op(B) = B)
 
 // CTA tile BM x BN, WM x WN warps, each warp owns (BM/WM) x (BN/WN) = MI m16 x NJ n8 MMA tiles.
-template <int BM_, int BN_, int WM_, int WN_>
+template <int BM_, int BN_, int WM_, int WN_, int ST_ = 4, int MINB_ = 1>
 struct Cfg {
-  static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_;
+  static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, STAGES = ST_, MINB = MINB_;
   static constexpr int MI = BM / WM / 16, NJ = BN / WN / 8;
   static constexpr int LDA_N = BM + 2;  // sA[k][m]  (op(A) = A)
   static constexpr int LDB_T = BN + 2;  // sB[k][n]  (op(B) = B^T)
   static_assert(WM * WN * 32 == NT, "8 warps");
   __host__ __device__ static constexpr int a_elems(bool ta) { return ta ? BM * LDA_T : BK * LDA_N; }
   __host__ __device__ static constexpr int b_elems(bool tb) { return tb ? BK * LDB_T : BN * LDB_N; }
-  static constexpr int smem(bool ta, bool tb) { return STAGES * (a_elems(ta) + b_elems(tb)) * 8; }
+  static constexpr int smem(bool ta, bool tb) { return ST_ * (a_elems(ta) + b_elems(tb)) * 8; }
 };
-using CfgBig = Cfg<128, 128, 2, 4>;   // general
-using CfgSkinnyM = Cfg<32, 128, 1, 8>;  // M <= 32 (V^T W products of the QR updates)
-using CfgSkinnyN = Cfg<128, 64, 4, 2>;  // N <= 64 (TRSM leaves, narrow updates)
+using CfgBig = Cfg<128, 128, 2, 4>;           // general: 1 CTA / SM, warp tile 64x32
+using CfgSkinnyM = Cfg<32, 64, 1, 8, 4, 3>;    // M <= 32 (V^T W products of the QR updates)
+using CfgSmall = Cfg<64, 64, 2, 4, 2, 3>;      // K <= 64 rank-k updates and N <= 64: 3 CTAs / SM
 
 struct KParams {
   GemmArgs g;
   int tiles_m, tiles_n;
   int splitk;
+  int preload;  // C loaded into the accumulators up front (rank-k updates)
   double* P;  // split-K partials
   int64_t ldp;
 };
 
 template <class C, bool TA, bool TB, bool V16>
-__global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
+__global__ void __launch_bounds__(NT, C::MINB) dgemm_kernel(KParams kp) {
   constexpr int BM = C::BM, BN = C::BN, MI = C::MI, NJ = C::NJ;
   constexpr int LDA_N = C::LDA_N, LDB_T = C::LDB_T;
   constexpr int AE = C::a_elems(TA), BE = C::b_elems(TB);
+  constexpr int STAGES = C::STAGES;
   extern __shared__ __align__(16) double smem[];
   const GemmArgs& p = kp.g;
   double* sAb = smem;
@@ -154,6 +156,36 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
       for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
   const int ktiles = (ke > kb) ? (ke - kb + BK - 1) / BK : 0;
+  // Rank-k updates C += alpha A B with |alpha| = 1 (the Householder and TRSM updates) are
+  // bound by streaming C: its tile is loaded into the accumulators before the MMAs, so the
+  // C reads overlap the A/B copies instead of following them.  C is pre-scaled by
+  // beta/alpha (exact for alpha = +-1) and the epilogue then writes alpha * acc.
+  const bool preload = kp.preload;
+  if (preload) {
+    const double* Cb = p.C + static_cast<int64_t>(bz) * p.strideC;
+    const double sc = p.beta / p.alpha;
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) {
+        const int r = m0 + wm + i * 16 + 2 * g;
+        const int c = n0 + wn + j * 8 + 2 * t;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int cc = c + h;
+          if (cc >= N || r >= M) continue;
+          const double* src = Cb + r + static_cast<int64_t>(cc) * p.ldc;
+          if (V16 && r + 1 < M) {
+            const double2 o = *reinterpret_cast<const double2*>(src);
+            acc[i][j][h] = sc * o.x;
+            acc[i][j][2 + h] = sc * o.y;
+          } else {
+            acc[i][j][h] = sc * src[0];
+            if (r + 1 < M) acc[i][j][2 + h] = sc * src[1];
+          }
+        }
+      }
+  }
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
     if (s < ktiles) load_stage(s, kb + s * BK);
@@ -236,7 +268,7 @@ __global__ void __launch_bounds__(NT, 1) dgemm_kernel(KParams kp) {
   double* C_ = p.C + static_cast<int64_t>(bz) * p.strideC;
   const int64_t ldc = p.ldc;
   const double alpha = p.alpha * (p.alpha_vec ? p.alpha_vec[bz] : 1.0);
-  const double beta = p.beta;
+  const double beta = preload ? 0.0 : p.beta;
 #pragma unroll
   for (int i = 0; i < MI; ++i)
 #pragma unroll
@@ -310,40 +342,58 @@ cudaError_t launch_c(const KParams& kp, dim3 grid, bool v16, cudaStream_t st) {
   return v16 ? launch_v<C, true>(kp, grid, st) : launch_v<C, false>(kp, grid, st);
 }
 
-// tile shape: 0 = 128x128, 1 = 32x128 (M <= 32), 2 = 128x64 (N <= 64)
+// tile shape: 0 = 128x128, 1 = 32x64 (M <= 32), 2 = 64x64 (K <= 64 or N <= 64)
 int pick_cfg(const GemmArgs& a) {
   if (a.tri) return 0;
   if (a.M <= 32) return 1;
-  if (a.N <= 64) return 2;
+  if (a.K <= 64 || a.N <= 64) return 2;
   return 0;
 }
 
-void tile_dims(int cfg, int* bm, int* bn) {
+void tile_dims(int cfg, int* bm, int* bn, int* per_sm) {
   if (cfg == 1) {
     *bm = CfgSkinnyM::BM;
     *bn = CfgSkinnyM::BN;
+    *per_sm = CfgSkinnyM::MINB;
   } else if (cfg == 2) {
-    *bm = CfgSkinnyN::BM;
-    *bn = CfgSkinnyN::BN;
+    *bm = CfgSmall::BM;
+    *bn = CfgSmall::BN;
+    *per_sm = CfgSmall::MINB;
   } else {
     *bm = CfgBig::BM;
     *bn = CfgBig::BN;
+    *per_sm = CfgBig::MINB;
   }
 }
 
+// Split K only when the tile grid cannot fill the GPU; pick the split that fills whole
+// waves (sms * resident CTAs per SM) best, with at least 8 K tiles per split.
 int choose_splitk(const GemmArgs& a, int sms) {
   if (a.splitk >= 1) return a.splitk;
-  int BM, BN;
-  tile_dims(pick_cfg(a), &BM, &BN);
+  int BM, BN, per_sm;
+  tile_dims(pick_cfg(a), &BM, &BN, &per_sm);
   const int tm = (a.M + BM - 1) / BM, tn = (a.N + BN - 1) / BN;
   const int64_t tiles = a.tri ? static_cast<int64_t>(tm) * (tm + 1) / 2 : static_cast<int64_t>(tm) * tn;
   const int64_t ctas = tiles * a.batch;
-  if (ctas >= sms) return 1;
+  const int64_t wave = static_cast<int64_t>(sms) * per_sm;
+  if (ctas >= wave) return 1;
   const int kt = (a.K + BK - 1) / BK;
-  int s = static_cast<int>((2 * sms + ctas - 1) / ctas);
-  s = std::min(s, kt / 8);
-  s = std::min(s, 32);
-  return std::max(s, 1);
+  const int smax = std::min(32, kt / 8);
+  if (smax < 2) return 1;
+  int best = 1;
+  double best_eff = static_cast<double>(ctas) / wave;  // fraction of one wave used unsplit
+  for (int s = 2; s <= smax; ++s) {
+    const int64_t c = ctas * s;
+    const int64_t waves = (c + wave - 1) / wave;
+    const double eff = static_cast<double>(c) / (waves * wave);  // wave fill
+    // prefer more parallelism until the first full wave, then fill
+    const double score = (c < wave ? static_cast<double>(c) / wave : eff) * (waves <= 3 ? 1.0 : 0.9);
+    if (score > best_eff + 1e-9) {
+      best_eff = score;
+      best = s;
+    }
+  }
+  return best;
 }
 
 }  // namespace
@@ -385,8 +435,8 @@ cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
   KParams kp;
   kp.g = a;
   const int cfg = pick_cfg(a);
-  int BM, BN;
-  tile_dims(cfg, &BM, &BN);
+  int BM, BN, per_sm;
+  tile_dims(cfg, &BM, &BN, &per_sm);
   kp.tiles_m = (a.M + BM - 1) / BM;
   kp.tiles_n = (a.N + BN - 1) / BN;
   kp.splitk = choose_splitk(a, sms);
@@ -400,12 +450,16 @@ cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
       kp.P = ws.ptr;
     }
   }
+  kp.preload = (kp.splitk <= 1 && a.beta != 0.0 && !a.tri && !a.alpha_vec && (a.alpha == 1.0 || a.alpha == -1.0) &&
+                a.K <= 64)
+                   ? 1
+                   : 0;
   const int64_t tiles = a.tri ? static_cast<int64_t>(kp.tiles_m) * (kp.tiles_m + 1) / 2
                               : static_cast<int64_t>(kp.tiles_m) * kp.tiles_n;
   if (tiles > 0x7fffffff || a.batch > 65535) return cudaErrorInvalidValue;
   dim3 grid(static_cast<unsigned>(tiles), kp.splitk, a.batch);
   const cudaError_t e = cfg == 1 ? launch_c<CfgSkinnyM>(kp, grid, v16, st)
-                        : cfg == 2 ? launch_c<CfgSkinnyN>(kp, grid, v16, st)
+                        : cfg == 2 ? launch_c<CfgSmall>(kp, grid, v16, st)
                                    : launch_c<CfgBig>(kp, grid, v16, st);
   if (e != cudaSuccess || kp.splitk <= 1) return e;
   const int64_t total = static_cast<int64_t>(a.M) * a.N;

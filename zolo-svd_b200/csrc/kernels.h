@@ -89,6 +89,8 @@ cudaError_t trtri_blocks(int n, const double* L, int64_t ldl, int64_t strideL, d
 cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, double* tau,
                      int64_t strideTau, double* T, int64_t strideT, double* Vexp, int64_t ldv,
                      int64_t strideV, int batch, cudaStream_t st);
+// Cluster size the panel kernel uses for an m x w panel (negative: rows stay in global memory).
+int qr_panel_config(int m, int w);
 // Vexp = unit-lower-trapezoidal V taken from A (m x w), batched.
 cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t strideA, double* V,
                       int64_t ldv, int64_t strideV, int batch, cudaStream_t st);

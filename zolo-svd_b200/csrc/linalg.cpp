@@ -45,7 +45,8 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   if (need) c.ensure_splitk(need);
   cudaStream_t s = st ? st : c.stream();
   Profiler::Rec rec;
-  if (c.prof.on) c.prof.begin(0, (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K * batch, s, &rec);
+  const int cls = tri ? 6 : (M <= 32 ? 3 : (N <= 64 ? 4 : (K <= 64 ? 5 : 0)));
+  if (c.prof.on) c.prof.begin(cls, (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K * batch, s, &rec);
   ck(dgemm(a, c.splitk(), s));
   if (c.prof.on) c.prof.end(rec, s);
   c.stats.launches += need ? 2 : 1;

@@ -3,17 +3,19 @@
 // dlarft conventions) on one thread-block cluster per panel.
 //
 // The m x w panel (w <= 32) is split by rows over the CL CTAs of a cluster;
-// each CTA keeps its rows in shared memory when they fit.  Column k costs ONE
-// pass over the CTA's rows and ONE cluster barrier:
-//   * the pass applies reflector k to the remaining columns and accumulates,
-//     in the same sweep, everything the next step needs: ||x_below||^2 and
-//     x_below . a_c of column k+1, and the Gram column V(:,0:k)^T v_k that
-//     the compact-WY factor T needs;
-//   * the 65 partial sums are block-reduced (warp reduce-scatter) into this
-//     CTA's shared memory; after the barrier every CTA gathers all CTAs'
-//     partials through distributed shared memory and sums them in the same
-//     fixed order, so all CTAs derive bit-identical beta / tau / v^T A and the
-//     same T column; partials are double-buffered by column parity.
+// each CTA keeps its rows in shared memory when they fit.  Inside a CTA the
+// work is column-parallel: thread (c, g) owns column c of the rows
+// r = g, g+8, g+16, ... of its chunk, so every phase is a short scalar loop
+// over independent rows and the row sums are 3 warp shuffles.  Column k costs
+// three CTA barriers and ONE cluster barrier:
+//   * gather: every CTA sums all CTAs' partials (||x_below||^2 and
+//     x_below . a_c) through distributed shared memory in the same fixed
+//     order, so all CTAs derive bit-identical beta / tau / v^T A;
+//   * update: columns c > k apply reflector k;
+//   * scale + dots: column k is scaled into v_k and the partials of column
+//     k+1 are formed and published (double-buffered by column parity).
+// The compact-WY factor T (dlarft) is formed once, after the last column, from
+// the cluster-wide V^T V.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -28,12 +30,13 @@ namespace zolo {
 namespace {
 
 constexpr int QW = 32;   // max panel width
-constexpr int QT = 256;  // threads per CTA
-constexpr int NWARP = QT / 32;
-constexpr int SLOT = 1 + 2 * QW;  // s0, d[QW], g[QW]
-constexpr int ROWK = SLOT;        // pivot row of the next column follows the partials
+constexpr int QT = 256;  // threads per CTA: 32 columns x 8 row groups
+constexpr int NG = 8;    // row groups
+constexpr int UB = 8;    // rows per load batch
+constexpr int UC = 16;   // columns per load batch in the update
+constexpr int SLOT = 1 + QW;  // s0, d[QW]
+constexpr int ROWK = SLOT;    // pivot row of the next column follows the partials
 constexpr int SLOT_ALL = SLOT + QW;
-constexpr int MAX_CL = 16;
 constexpr size_t SMEM_CHUNK_CAP = 190 * 1024;
 
 struct PanelArgs {
@@ -48,28 +51,21 @@ struct PanelArgs {
   int64_t ldv, strideV;
 };
 
-// after the call lane l holds in v[0] the warp sum of value index l
-ZDEV void warp_reduce_scatter32(double (&v)[QW], int lane) {
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    const bool up = lane & o;
-#pragma unroll
-    for (int i = 0; i < o; ++i) {
-      const double send = up ? v[i] : v[i + o];
-      const double keep = up ? v[i + o] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-    }
-  }
+ZDEV double group_sum8(double v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  return v;
 }
 
 struct PanelShared {
   double part[2][SLOT_ALL];
-  double red[NWARP][SLOT];
-  double gat[MAX_CL][SLOT];
   double sum[SLOT];
   double rowk[QW];
   double colk[QW];
   double tauv[QW];
+  double G[QW * QW];   // this CTA's partial V^T V (upper triangle)
+  double Gs[QW * QW];  // rank 0: cluster sum of G
   double T[QW * QW];
 };
 
@@ -90,97 +86,75 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
   const int r0 = rank * p.rows_per;
   const int r1 = min(m, r0 + p.rows_per);
   const int nloc = max(r1 - r0, 0);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int col = (tid >> 5) * 4 + (lane >> 3);  // column owned by this thread
+  const int grp = lane & 7;                      // row group: local rows grp, grp+8, ...
   const int rp = p.rp_ld;
 
-  // element (local row rl of this CTA, column c) of the panel
   auto at = [&](int rl, int c) -> double& {
     if (SMEM) return chunk[c * rp + rl];
     return A[(r0 + rl) + c * lda];
   };
-
-  if (SMEM) {
-    for (int c = 0; c < w; ++c)
-      for (int rl = tid; rl < nloc; rl += QT) chunk[c * rp + rl] = A[(r0 + rl) + c * lda];
-  }
-  for (int e = tid; e < QW * QW; e += QT) S.T[e] = 0.0;
-
-  double acc_s0;
-  double accd[QW], accg[QW];
-
-  auto reduce_and_publish = [&](double* out) {
-    const double s0w = warp_sum(acc_s0);
-    warp_reduce_scatter32(accd, lane);
-    warp_reduce_scatter32(accg, lane);
-    if (lane == 0) S.red[warp][0] = s0w;
-    S.red[warp][1 + lane] = accd[0];
-    S.red[warp][1 + QW + lane] = accg[0];
-    __syncthreads();
-    if (tid < SLOT) {
-      double s = 0.0;
+  // first local row >= global row `from` that belongs to this thread's group
+  auto first_row = [&](int from) {
+    int rl = max(from - r0, 0);
+    rl += (grp - rl % NG + NG) % NG;
+    return rl;
+  };
+  // sum over this thread's rows (from rl0) of a(r, x) * a(r, col): batches of UB rows whose
+  // loads are all issued first, four independent partial sums
+  auto dot_rows = [&](int rl0, int x) {
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int rl = rl0; rl < nloc; rl += NG * UB) {
+      double xa[UB], xb[UB];
 #pragma unroll
-      for (int q = 0; q < NWARP; ++q) s += S.red[q][tid];
-      out[tid] = s;
+      for (int u = 0; u < UB; ++u) {
+        const int r = rl + u * NG;
+        xa[u] = (r < nloc) ? at(r, x) : 0.0;
+        xb[u] = (r < nloc) ? at(r, col) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < UB; ++u) s4[u & 3] += xa[u] * xb[u];
     }
+    return (s4[0] + s4[1]) + (s4[2] + s4[3]);
   };
 
-  // ---- partials for column 0 ----
-  acc_s0 = 0.0;
-#pragma unroll
-  for (int c = 0; c < QW; ++c) accd[c] = accg[c] = 0.0;
-  __syncthreads();
-  for (int rl = tid; rl < nloc; rl += QT) {
-    const int r = r0 + rl;
-    const double x = at(rl, 0);
-    if (r > 0) {
-      acc_s0 += x * x;
-#pragma unroll
-      for (int c = 1; c < QW; ++c)
-        if (c < w) accd[c] += x * at(rl, c);
-    } else {
-#pragma unroll
-      for (int c = 0; c < QW; ++c)
-        if (c < w) S.part[0][ROWK + c] = at(rl, c);
+  if (SMEM) {
+    const int tot = w * nloc;
+    for (int e = tid; e < tot; e += QT) {
+      const int c = e / nloc, rl = e - c * nloc;
+      chunk[c * rp + rl] = A[(r0 + rl) + c * lda];
     }
   }
-  reduce_and_publish(S.part[0]);
+  __syncthreads();
+
+  // ---- partials of column 0 ----
+  {
+    double acc = 0.0;
+    if (col < w) {
+      acc = dot_rows(first_row(1), 0);  // col 0: ||x_below||^2
+      if (r0 == 0 && grp == 0 && nloc > 0) S.part[0][ROWK + col] = at(0, col);  // pivot row 0
+    }
+    acc = group_sum8(acc);
+    if (grp == 0 && col < w) S.part[0][col == 0 ? 0 : 1 + col] = acc;
+  }
   cluster.sync();
 
-  for (int k = 0; k <= w; ++k) {
+  for (int k = 0; k < w; ++k) {
     const int buf = k & 1;
-    // ---- gather the partials of all CTAs (one remote load per element) ----
-    for (int e = tid; e < CL * SLOT; e += QT) {
-      const int q = e / SLOT, i = e - q * SLOT;
-      S.gat[q][i] = cluster.map_shared_rank(&S.part[buf][0], q)[i];
-    }
-    if (k < w) {
-      const int owner = k / p.rows_per;
-      if (tid < w) S.rowk[tid] = cluster.map_shared_rank(&S.part[buf][0], owner)[ROWK + tid];
-    }
-    __syncthreads();
+    // ---- gather: thread i < SLOT sums entry i over all CTAs (same order everywhere) ----
     if (tid < SLOT) {
       double s = 0.0;
-      for (int q = 0; q < CL; ++q) s += S.gat[q][tid];
+      for (int q = 0; q < CL; ++q) s += cluster.map_shared_rank(&S.part[buf][0], q)[tid];
       S.sum[tid] = s;
+    } else if (tid < SLOT + w) {
+      const int owner = k / p.rows_per;
+      const int c = tid - SLOT;
+      S.rowk[c] = cluster.map_shared_rank(&S.part[buf][0], owner)[ROWK + c];
     }
     __syncthreads();
-    // ---- T column k-1 from the Gram column g = V(:,0:k-1)^T v_{k-1} (dlarft) ----
-    if (k > 0) {
-      const int kc = k - 1;
-      const double tk = S.tauv[kc];
-      double tv = 0.0;
-      if (tid < kc) {
-        for (int j = tid; j < kc; ++j) tv += S.T[tid + j * QW] * S.sum[1 + QW + j];
-        tv = -tk * tv;
-      }
-      __syncthreads();
-      if (tid < kc) S.T[tid + kc * QW] = tv;
-      if (tid == 0) S.T[kc + kc * QW] = tk;
-      __syncthreads();
-    }
-    if (k == w) break;
 
-    // ---- reflector k (dlarfg) ----
+    // ---- reflector k (dlarfg), computed redundantly and identically by every thread ----
     const double s0 = S.sum[0];
     const double alpha = S.rowk[k];
     double beta, tau, scal;
@@ -200,66 +174,147 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
     }
     __syncthreads();
 
-    // ---- apply reflector k; accumulate partials of column k+1 and the Gram column of v_k ----
-    acc_s0 = 0.0;
+    // ---- update: a(r,c) -= tau * v_r * (v^T a_c) for c > k, rows r >= k ----
+    // each thread owns whole rows and loads a batch of UC columns before storing any
+    // (a store may alias the next loads of the same array, so batching is explicit)
+    for (int rl = max(k - r0, 0) + tid; rl < nloc; rl += QT) {
+      const double tv = tau * ((r0 + rl == k) ? 1.0 : at(rl, k) * scal);
+      for (int c0 = k + 1; c0 < w; c0 += UC) {
+        double xc[UC];
 #pragma unroll
-    for (int c = 0; c < QW; ++c) accd[c] = accg[c] = 0.0;
-    const int nk = k + 1;
-    for (int rl = tid; rl < nloc; rl += QT) {
-      const int r = r0 + rl;
-      if (r < k) {
-        V[r + k * ldv] = 0.0;
-        continue;
-      }
-      if (r == k) {
-        at(rl, k) = beta;
-        V[r + k * ldv] = 1.0;
+        for (int u = 0; u < UC; ++u)
+          if (c0 + u < w) xc[u] = at(rl, c0 + u);
 #pragma unroll
-        for (int c = 0; c < QW; ++c) {
-          if (c > k && c < w) at(rl, c) -= tau * S.colk[c];
-          if (c < k) accg[c] += at(rl, c);  // V(k, c) * 1
-        }
-        if (nk < w) {
-#pragma unroll
-          for (int c = 0; c < QW; ++c)
-            if (c >= nk && c < w) S.part[buf ^ 1][ROWK + c] = at(rl, c);
-        }
-        continue;
-      }
-      const double v = at(rl, k) * scal;
-      at(rl, k) = v;
-      V[r + k * ldv] = v;
-      double xn = 0.0;
-#pragma unroll
-      for (int c = 0; c < QW; ++c) {
-        if (c < k) {
-          accg[c] += at(rl, c) * v;
-        } else if (c > k && c < w) {
-          const double a = at(rl, c) - tau * v * S.colk[c];
-          at(rl, c) = a;
-          if (c == nk) {
-            xn = a;
-            if (r > nk) acc_s0 += a * a;
-          } else if (r > nk) {
-            accd[c] += xn * a;
-          }
-        }
-      }
-      if (r == nk && nk < w) {
-#pragma unroll
-        for (int c = 0; c < QW; ++c)
-          if (c >= nk && c < w) S.part[buf ^ 1][ROWK + c] = at(rl, c);
+        for (int u = 0; u < UC; ++u)
+          if (c0 + u < w) at(rl, c0 + u) = xc[u] - tv * S.colk[c0 + u];
       }
     }
-    reduce_and_publish(S.part[buf ^ 1]);
+    __syncthreads();
+
+    // ---- scale column k into v_k (all threads); partials of column k+1 (column threads) ----
+    const int nk = k + 1;
+    for (int base = tid; base < nloc; base += QT * UB) {
+      double x[UB];
+#pragma unroll
+      for (int u = 0; u < UB; ++u) {
+        const int rl = base + u * QT;
+        if (rl < nloc && r0 + rl > k) x[u] = at(rl, k);
+      }
+#pragma unroll
+      for (int u = 0; u < UB; ++u) {
+        const int rl = base + u * QT;
+        if (rl >= nloc) continue;
+        const int r = r0 + rl;
+        double v;
+        if (r < k) {
+          v = 0.0;
+        } else if (r == k) {
+          at(rl, k) = beta;
+          v = 1.0;
+        } else {
+          v = x[u] * scal;
+          at(rl, k) = v;
+        }
+        V[r + k * ldv] = v;
+      }
+    }
+    double acc = 0.0;
+    if (nk < w && col >= nk && col < w) {
+      acc = dot_rows(first_row(nk + 1), nk);
+      const int lr = nk - r0;  // pivot row of column k+1, if this CTA holds it
+      if (lr >= 0 && lr < nloc && grp == lr % NG) S.part[buf ^ 1][ROWK + col] = at(lr, col);
+    }
+    acc = group_sum8(acc);
+    if (nk < w && grp == 0 && col >= nk && col < w) S.part[buf ^ 1][col == nk ? 0 : 1 + col] = acc;
     cluster.sync();
   }
 
-  if (SMEM) {
-    for (int c = 0; c < w; ++c)
-      for (int rl = tid; rl < nloc; rl += QT) A[(r0 + rl) + c * lda] = chunk[c * rp + rl];
+  // ---- V^T V of this CTA's rows on the FP64 tensor path: warp q takes rows q, q+8k8 ...
+  // V(r,i) = a(r,i) below the diagonal, 1 on it, 0 above; the 32 x 32 partials of the 8
+  // warps are summed through shared memory into G ----
+  {
+    const int warp = tid >> 5;
+    const int gq = lane >> 2, tq = lane & 3;
+    auto vval = [&](int rl, int i) -> double {
+      const int r = r0 + rl;
+      if (rl >= nloc || i >= w || r < i) return 0.0;
+      return (r == i) ? 1.0 : at(rl, i);
+    };
+    double accg[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 4; ++bb)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) accg[a][bb][r] = 0.0;
+    // k8 steps of rows: step s covers local rows 8s .. 8s+7; warp q does steps q, q+8, ...
+    for (int st = warp; st * 8 < nloc; st += QT / 32) {
+      const int rb = st * 8;
+      double af[2][4], bf[4][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {  // A = V^T: rows i, k = local row
+        const int i0 = a * 16 + gq;
+        af[a][0] = vval(rb + tq, i0);
+        af[a][1] = vval(rb + tq, i0 + 8);
+        af[a][2] = vval(rb + tq + 4, i0);
+        af[a][3] = vval(rb + tq + 4, i0 + 8);
+      }
+#pragma unroll
+      for (int bb = 0; bb < 4; ++bb) {  // B = V: k = local row, n = j
+        const int j0 = bb * 8 + gq;
+        bf[bb][0] = vval(rb + tq, j0);
+        bf[bb][1] = vval(rb + tq + 4, j0);
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) dmma_16x8x8(accg[a][bb], af[a], bf[bb]);
+    }
+    for (int e = tid; e < QW * QW; e += QT) S.G[e] = 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 4; ++bb) {
+        const int i = a * 16 + gq, j = bb * 8 + 2 * tq;
+        atomicAdd(&S.G[i + j * QW], accg[a][bb][0]);
+        atomicAdd(&S.G[i + (j + 1) * QW], accg[a][bb][1]);
+        atomicAdd(&S.G[i + 8 + j * QW], accg[a][bb][2]);
+        atomicAdd(&S.G[i + 8 + (j + 1) * QW], accg[a][bb][3]);
+      }
   }
+  if (SMEM) {
+    const int tot = w * nloc;
+    for (int e = tid; e < tot; e += QT) {
+      const int c = e / nloc, rl = e - c * nloc;
+      A[(r0 + rl) + c * lda] = chunk[c * rp + rl];
+    }
+  }
+  cluster.sync();
   if (rank == 0) {
+    // T(k,k) = tau_k, T(0:k,k) = -tau_k T(0:k,0:k) V(:,0:k)^T v_k  (dlarft, forward, columnwise)
+    for (int e = tid; e < QW * QW; e += QT) {
+      double gq[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) gq[q] = (q < CL) ? cluster.map_shared_rank(S.G, q)[e] : 0.0;
+      double g = 0.0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) g += gq[q];
+      S.Gs[e] = g;
+      S.T[e] = 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < w; ++k) {
+      const double tk = S.tauv[k];
+      if (tid < k) {
+        double tv = 0.0;
+        for (int j = tid; j < k; ++j) tv += S.T[tid + j * QW] * S.Gs[j + k * QW];
+        S.T[tid + k * QW] = -tk * tv;
+      } else if (tid == k) {
+        S.T[k + k * QW] = tk;
+      }
+      __syncthreads();
+    }
     double* T = p.T + b * p.strideT;
     for (int e = tid; e < QW * QW; e += QT) T[e] = S.T[e];
   }
@@ -370,6 +425,16 @@ int max_cluster() {
 
 }  // namespace
 
+int qr_panel_config(int m, int w) {
+  const int maxcl = max_cluster();
+  int cl = 1;
+  while (cl < maxcl && (static_cast<size_t>(((m + cl - 1) / cl + 7) / 16 * 16 + 8) * w * 8 > SMEM_CHUNK_CAP ||
+                        (m + cl - 1) / cl > 512))
+    cl *= 2;
+  const size_t chunk = static_cast<size_t>(((m + cl - 1) / cl + 7) / 16 * 16 + 8) * w * 8;
+  return chunk <= SMEM_CHUNK_CAP ? cl : -cl;
+}
+
 cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, double* tau, int64_t strideTau,
                      double* T, int64_t strideT, double* Vexp, int64_t ldv, int64_t strideV, int batch,
                      cudaStream_t st) {
@@ -378,14 +443,14 @@ cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, doub
   const int maxcl = max_cluster();
   // smallest cluster whose per-CTA row chunk fits in shared memory, with at most ~512 rows per CTA
   int cl = 1;
-  while (cl < maxcl && (static_cast<size_t>(((m + cl - 1) / cl) | 1) * w * 8 > SMEM_CHUNK_CAP ||
+  while (cl < maxcl && (static_cast<size_t>(((m + cl - 1) / cl + 7) / 16 * 16 + 8) * w * 8 > SMEM_CHUNK_CAP ||
                         (m + cl - 1) / cl > 512))
     cl *= 2;
   PanelArgs pa;
   pa.m = m;
   pa.w = w;
   pa.rows_per = (m + cl - 1) / cl;
-  pa.rp_ld = pa.rows_per | 1;  // odd stride
+  pa.rp_ld = (pa.rows_per + 7) / 16 * 16 + 8;  // = 8 mod 16: conflict-free half-warp access
   pa.A = A;
   pa.lda = lda;
   pa.strideA = strideA;
