@@ -109,6 +109,16 @@ void zolo_pzolopd1(char sym, int rk, int m, int n, double alpha, double beta, co
 void zolo_pzolopd2(char sym, int rk, int m, int n, double alpha, double beta, const double* as, int ia, int ja,
                    const int* desca, double* q, int iq, int jq, const int* descq, int* info, char polar);
 
+/* ZoloEig (ZoloEig.f90:2): partial eigendecomposition of the symmetric N x N matrix As
+ * from Q = polar factor of As - sigma*I: the Rk = round(||(Q - I)/2||_F^2) eigenpairs
+ * below sigma (PQDWHSUBIT subspace iteration, pqdwhsubit.f90:227-312, then an
+ * eigensolve of the leading Rk block).  On exit, as in the reference: Q = the subspace
+ * basis V (N x N), As = V^T As V, TAU(1:Rk) = eigenvalues (ascending),
+ * WORK(1:N*Rk) = eigenvectors (leading dimension N).  CONTXT and MPI_NEWCOMM are
+ * ignored (1x1 grid); NBLK is not used.  LWORK >= N*N and LWORK2 >= N*N. */
+void zolo_zoloeig(int n, int nblk, double* q, double* as, int contxt, int mpi_newcomm, double* work, int lwork,
+                  double* work2, int lwork2, double* tau, int* info);
+
 /* gfortran-mangled aliases: all arguments by reference, hidden CHARACTER lengths last */
 void pqdwhfacs_(const char* sym, const int* m, const int* n, const double* sigma, const double* a, const int* ia,
                 const int* ja, const int* desca, double* q, const int* iq, const int* jq, const int* descq,
@@ -121,6 +131,8 @@ void zolopd_(const int* m, const int* n, const double* sigma, const double* a, c
 void pzolopd1_(const char* sym, const int* rk, const int* m, const int* n, const double* alpha, const double* beta,
                const double* as, const int* ia, const int* ja, const int* desca, double* q, const int* iq,
                const int* jq, const int* descq, int* info, const char* polar, size_t sym_len, size_t polar_len);
+void zoloeig_(const int* n, const int* nblk, double* q, double* as, const int* contxt, const int* mpi_newcomm,
+              double* work, const int* lwork, double* work2, const int* lwork2, double* tau, int* info);
 void pzolopd2_(const char* sym, const int* rk, const int* m, const int* n, const double* alpha, const double* beta,
                const double* as, const int* ia, const int* ja, const int* desca, double* q, const int* iq,
                const int* jq, const int* descq, int* info, const char* polar, size_t sym_len, size_t polar_len);
@@ -142,6 +154,20 @@ int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* d
 /* H = (Q^T A + A^T Q)/2 (pqdwhfacs.f90:460-466, ZoloCHK1.f90:80-83). */
 int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda,
                     double* dH, int64_t ldh);
+
+/* Symmetric eigendecomposition H = Z diag(w) Z^T (n x n), w ascending: the replacement
+ * of ELPA_PDSYEVD2 (elpa_pdsyevd2.F90:199-200) -- spectral divide-and-conquer on the
+ * polar decomposition (QDWH of H - sigma I, subspace split as pqdwhsubit.f90:227-312,
+ * recursively) with batched Jacobi leaves.  Returns 0, or > 0 if no split point worked. */
+int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz);
+/* Zolo-SVD (test_zolodrv1.f90 + ZoloCHK1.f90:80-91): A = U diag(s) V^T for m >= n via
+ * QDWH-PD (algo 0) or Zolo-PD with rk terms (algo 1), H = sym(Q^T A), H = V diag(s) V^T,
+ * U = Q V.  s ascending (the order ZoloCHK1 receives from ELPA). */
+int zolo_svd_dev(zolo_handle_t h, int algo, int rk, int m, int n, const double* dA, int64_t lda, double* dU,
+                 int64_t ldu, double* dS, double* dV, int64_t ldv);
+/* ZoloEig on device arrays: *rk eigenpairs of A below the shift used to form Q. */
+int zolo_zoloeig_dev(zolo_handle_t h, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, int* rk,
+                     double* dW, double* dZ, int64_t ldz);
 
 /* ---- kernel-level entry points (building blocks, used by the parity tests) ---- */
 /* C = alpha op(A) op(B) + beta C (PDGEMM on a 1x1 grid); tri = lower-triangle-only output,

@@ -112,11 +112,18 @@ _SIGS = [
     ("zolo_formx2_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64, C.c_void_p,
                                   C.c_int64, c_double_p]),
     ("zolo_dpotrf_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_int64, C.c_void_p]),
+    ("zolo_syev_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64]),
+    ("zolo_svd_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                               C.c_int64, C.c_void_p, C.c_void_p, C.c_int64]),
+    ("zolo_zoloeig_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, c_int_p,
+                                   C.c_void_p, C.c_void_p, C.c_int64]),
+    ("zolo_zoloeig", None, [C.c_int, C.c_int, c_double_p, c_double_p, C.c_int, C.c_int, c_double_p, C.c_int,
+                            c_double_p, C.c_int, c_double_p, c_int_p]),
 ]
 
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
-EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_"]
+EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
 
 
 class ZoloError(RuntimeError):
@@ -329,6 +336,34 @@ def pzolopd1_dev(h: Handle, sym: str, rk: int, m: int, n: int, alpha: float, bet
                  dQ: int, ldq: int, dH: int = 0, ldh: int = 1) -> int:
     return _ck("zolo_pzolopd1_dev", lib().zolo_pzolopd1_dev(h.ptr, sym.encode()[:1], rk, m, n, alpha, beta, dA, lda,
                                                            dQ, ldq, dH or None, ldh))
+
+
+def syev_dev(h: Handle, n: int, dH: int, ldh: int, dW: int, dZ: int, ldz: int) -> int:
+    """Symmetric eigendecomposition (ascending) on device arrays."""
+    return _ck("zolo_syev_dev", lib().zolo_syev_dev(h.ptr, n, dH, ldh, dW, dZ, ldz))
+
+
+def svd_dev(h: Handle, m: int, n: int, dA: int, lda: int, dU: int, ldu: int, dS: int, dV: int, ldv: int,
+            algo: int = 0, rk: int = 8) -> int:
+    """A = U diag(s) V^T (s ascending) via QDWH-PD (algo 0) or Zolo-PD (algo 1) + eigensolve of H."""
+    return _ck("zolo_svd_dev", lib().zolo_svd_dev(h.ptr, algo, rk, m, n, dA, lda, dU, ldu, dS, dV, ldv))
+
+
+def zoloeig(q: np.ndarray, a: np.ndarray, nblk: int = 64):
+    """ZoloEig on host arrays: returns (eigenvalues, eigenvectors, V, V^T A V, INFO)."""
+    a = np.asfortranarray(a, dtype=np.float64).copy(order="F")
+    q = np.asfortranarray(q, dtype=np.float64).copy(order="F")
+    n = a.shape[0]
+    work = np.zeros(max(n * n, 1))
+    work2 = np.zeros(max(n * n, 1))
+    tau = np.zeros(max(n, 1))
+    info = C.c_int(0)
+    q_in = q.copy(order="F")
+    lib().zolo_zoloeig(n, nblk, _dp(q), _dp(a), 0, 0, _dp(work), len(work), _dp(work2), len(work2), _dp(tau),
+                       C.byref(info))
+    rk = int(round(float(np.linalg.norm((q_in - np.eye(n)) / 2.0) ** 2))) if n else 0
+    vecs = work[: n * rk].reshape((n, rk), order="F")
+    return tau[:rk].copy(), vecs.copy(), q, a, info.value
 
 
 def bounds_dev(h: Handle, m: int, n: int, dA: int, lda: int, mode: int = 1, sigma: float = 0.0):

@@ -13,6 +13,7 @@
 
 #include "coeff.h"
 #include "context.h"
+#include "eig.h"
 #include "linalg.h"
 #include "polar.h"
 
@@ -366,6 +367,77 @@ int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq
     zolo::ck(cudaStreamSynchronize(c.stream()));
     return 0;
   });
+}
+
+int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz) {
+  if (n < 0) return -2;
+  return guarded(h, [&](Context& c) {
+    zolo::EigStats es;
+    const int info = zolo::syev_dc(c, n, dH, ldh, dW, dZ, ldz, &es);
+    c.stats = zolo::Stats{};
+    c.stats.iterations = es.splits;
+    c.stats.qr_iterations = es.qdwh_iterations;
+    c.stats.chol_iterations = es.leaves;
+    c.stats.last_err = es.max_split_residual;
+    c.stats.flops = es.flops;
+    return info;
+  });
+}
+
+int zolo_svd_dev(zolo_handle_t h, int algo, int rk, int m, int n, const double* dA, int64_t lda, double* dU,
+                 int64_t ldu, double* dS, double* dV, int64_t ldv) {
+  if (m < n) return -4;
+  if (algo == 1 && (rk < 1 || rk > 8)) return -3;
+  return guarded(h, [&](Context& c) { return zolo::svd(c, m, n, dA, lda, algo, rk, dU, ldu, dS, dV, ldv, nullptr); });
+}
+
+int zolo_zoloeig_dev(zolo_handle_t h, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, int* rk,
+                     double* dW, double* dZ, int64_t ldz) {
+  if (n < 0) return -2;
+  return guarded(h, [&](Context& c) {
+    return zolo::zoloeig(c, n, dQ, ldq, dA, lda, rk, dW, dZ, ldz, nullptr, 0, nullptr, 0);
+  });
+}
+
+void zolo_zoloeig(int n, int /*nblk*/, double* q, double* as, int /*contxt*/, int /*mpi_newcomm*/, double* work,
+                  int lwork, double* /*work2*/, int lwork2, double* tau, int* info) {
+  int r = 0;
+  if (n < 0) r = -1;
+  else if (lwork < n * n) r = -8;
+  else if (lwork2 < n * n) r = -10;
+  if (r == 0 && n > 0) {
+    zolo_handle_t h = nullptr;
+    r = zolo_default_handle(&h);
+    if (r == 0)
+      r = guarded(h, [&](Context& c) -> int {
+        DevBuf dQ, dA, dV, dE, dW, dZ;
+        const size_t nn = static_cast<size_t>(n) * n;
+        zolo::ck(cudaMalloc(&dQ.p, nn * 8));
+        zolo::ck(cudaMalloc(&dA.p, nn * 8));
+        zolo::ck(cudaMalloc(&dV.p, nn * 8));
+        zolo::ck(cudaMalloc(&dE.p, nn * 8));
+        zolo::ck(cudaMalloc(&dW.p, static_cast<size_t>(n) * 8));
+        zolo::ck(cudaMalloc(&dZ.p, nn * 8));
+        zolo::ck(cudaMemcpyAsync(dQ.p, q, nn * 8, cudaMemcpyHostToDevice, c.stream()));
+        zolo::ck(cudaMemcpyAsync(dA.p, as, nn * 8, cudaMemcpyHostToDevice, c.stream()));
+        int rk = 0;
+        const int inf = zolo::zoloeig(c, n, dQ.p, n, dA.p, n, &rk, dW.p, dZ.p, n, dV.p, n, dE.p, n);
+        if (inf == 0 && rk > 0 && rk < n) {
+          zolo::ck(cudaMemcpyAsync(q, dV.p, nn * 8, cudaMemcpyDeviceToHost, c.stream()));
+          zolo::ck(cudaMemcpyAsync(as, dE.p, nn * 8, cudaMemcpyDeviceToHost, c.stream()));
+          zolo::ck(cudaMemcpyAsync(tau, dW.p, static_cast<size_t>(rk) * 8, cudaMemcpyDeviceToHost, c.stream()));
+          zolo::ck(cudaMemcpyAsync(work, dZ.p, static_cast<size_t>(n) * rk * 8, cudaMemcpyDeviceToHost, c.stream()));
+        }
+        zolo::ck(cudaStreamSynchronize(c.stream()));
+        return inf;
+      });
+  }
+  if (info) *info = r;
+}
+
+void zoloeig_(const int* n, const int* nblk, double* q, double* as, const int* contxt, const int* mpi_newcomm,
+              double* work, const int* lwork, double* work2, const int* lwork2, double* tau, int* info) {
+  zolo_zoloeig(*n, *nblk, q, as, *contxt, *mpi_newcomm, work, *lwork, work2, *lwork2, tau, info);
 }
 
 int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,

@@ -1,0 +1,321 @@
+// Symmetric eigensolver by spectral divide-and-conquer on the polar
+// decomposition (the reference's QDWH-eig split of pqdwheig.f90:168-228 /
+// ZoloEig.f90:78-102 / pqdwhsubit.f90:227-312, applied recursively), with a
+// batched Jacobi kernel at the leaves; ZoloEig; and the Zolo-SVD assembly of
+// ZoloCHK1.f90:80-91 (H = sym(Q^T A), H = Z diag(w) Z^T, U = Q Z).
+#include "eig.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "linalg.h"
+#include "polar.h"
+
+namespace zolo {
+
+namespace {
+
+inline int64_t even(int64_t x) { return (x + 1) / 2 * 2; }
+
+struct DevMem {
+  std::vector<void*> ptrs;
+  double* alloc(size_t elems) {
+    void* p = nullptr;
+    ck(cudaMalloc(&p, std::max<size_t>(elems, 1) * sizeof(double)));
+    ptrs.push_back(p);
+    return static_cast<double*>(p);
+  }
+  void release(double* p) {
+    for (auto& q : ptrs)
+      if (q == p) {
+        cudaFree(q);
+        q = nullptr;
+      }
+  }
+  ~DevMem() {
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+double d2h(Context& c, const double* d) {
+  double v = 0.0;
+  ck(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  return v;
+}
+
+struct Node {
+  int n = 0;
+  double* H = nullptr;  // node matrix (n x n, ld ldn)
+  int64_t ld = 0;
+  double* V = nullptr;  // split basis [V1 V2]
+  double* Z = nullptr;  // eigenvectors
+  double* w = nullptr;  // eigenvalues
+  int k = 0;
+  int left = -1, right = -1;
+  bool leaf = false;
+};
+
+// Orthonormal basis of range(P) completed to an n x n orthogonal V = [V1 V2]:
+// V from the Householder QR of X (n x k) with all n columns formed.
+void basis_from(Context& c, int n, int k, Mat X, double* V, int64_t ldv) {
+  double* tau = c.buf("eig_tau", k);
+  double* T = c.buf("eig_t", static_cast<size_t>((k + 31) / 32) * 1024);
+  geqrf(c, n, k, -1, X, tau, T, 1);
+  orgqr(c, n, k, -1, X, T, Mat{V, ldv, 0}, 1, n);
+}
+
+// off = ||E(k:n, 0:k)||_F for E = V^T H V (E returned)
+double split_residual(Context& c, int n, int k, const double* H, int64_t ldh, const double* V, int64_t ldv, double* E,
+                      int64_t lde) {
+  const int64_t ldn = even(n);
+  double* HV = c.buf("eig_hv", static_cast<size_t>(ldn) * n);
+  gemm(c, 0, 0, n, n, n, 1.0, Mat{const_cast<double*>(H), ldh, 0}, Mat{const_cast<double*>(V), ldv, 0}, 0.0,
+       Mat{HV, ldn, 0}, 1);
+  gemm(c, 1, 0, n, n, n, 1.0, Mat{const_cast<double*>(V), ldv, 0}, Mat{HV, ldn, 0}, 0.0, Mat{E, lde, 0}, 1);
+  ck(frob2(n - k, k, E + k, lde, c.dpartial(), c.dscal() + 8, c.stream()));
+  return std::sqrt(d2h(c, c.dscal() + 8));
+}
+
+}  // namespace
+
+int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz, EigStats* es) {
+  if (n <= 0) return 0;
+  EigStats local;
+  EigStats& S = es ? *es : local;
+  S = EigStats{};
+  DevMem mem;
+  std::vector<Node> nodes;
+  {
+    Node root;
+    root.n = n;
+    root.ld = even(n);
+    root.H = mem.alloc(static_cast<size_t>(root.ld) * n);
+    ck(scale_copy(n, n, 1.0, dH, ldh, 0, root.H, root.ld, 0, 1, 0.0, c.stream()));
+    nodes.push_back(root);
+  }
+  double hnorm;
+  ck(frob2(n, n, nodes[0].H, nodes[0].ld, c.dpartial(), c.dscal() + 9, c.stream()));
+  hnorm = std::sqrt(d2h(c, c.dscal() + 9));
+  // accepted leak ||V2^T H V1||_F of a split (the dropped block is the eigen-residual it adds)
+  const double eps = 2.220446049250313e-16;
+
+  // ---- top-down splits ----
+  for (size_t ni = 0; ni < nodes.size(); ++ni) {
+    Node nd = nodes[ni];
+    const int m = nd.n;
+    const int64_t ldm = even(m);
+    nd.Z = mem.alloc(static_cast<size_t>(ldm) * m);
+    nd.w = mem.alloc(m);
+    if (m <= kJacobiLeaf) {
+      nd.leaf = true;
+      nodes[ni] = nd;
+      continue;
+    }
+    // split points: median and mean of the diagonal, then nudged versions
+    std::vector<double> dg(m);
+    double* dd = c.buf("eig_diag", m);
+    ck(get_diag(m, nd.H, nd.ld, dd, c.stream()));
+    ck(cudaMemcpyAsync(dg.data(), dd, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream()));
+    ck(cudaStreamSynchronize(c.stream()));
+    std::vector<double> srt = dg;
+    std::sort(srt.begin(), srt.end());
+    const double med = srt[m / 2], mean = std::accumulate(dg.begin(), dg.end(), 0.0) / m;
+    const double span = std::max(srt.back() - srt.front(), 1e-300);
+    const double cand[4] = {0.5 * (srt[(m - 1) / 2] + srt[m / 2]), mean, med + 1e-3 * span, med - 1e-3 * span};
+    nd.V = mem.alloc(static_cast<size_t>(ldm) * m);
+    double* Up = c.buf("eig_up", static_cast<size_t>(ldm) * m);
+    double* P = c.buf("eig_p", static_cast<size_t>(ldm) * m);
+    double* X = c.buf("eig_x", static_cast<size_t>(ldm) * m);
+    double* E = c.buf("eig_e", static_cast<size_t>(ldm) * m);
+    bool ok = false;
+    for (int a = 0; a < 4 && !ok; ++a) {
+      QdwhOpts o;
+      o.sym = 'N';
+      o.sigma = cand[a];
+      o.bounds = BOUNDS_PQDWHFACS;
+      o.maxit = 12;
+      const Stats saved = c.stats;
+      const int info = qdwh(c, m, m, nd.H, nd.ld, Up, ldm, nullptr, 0, o);
+      S.qdwh_calls++;
+      S.qdwh_iterations += c.stats.iterations;
+      S.flops += c.stats.flops;
+      c.stats = saved;
+      if (info != 0) continue;
+      // projector onto the eigenvalues above the split: P = (Up + I)/2, k = trace(P)
+      ck(scale_copy(m, m, 0.5, Up, ldm, 0, P, ldm, 0, 1, 0.5, c.stream()));
+      ck(trace(m, P, ldm, c.dscal() + 10, c.stream()));
+      const int k = static_cast<int>(std::lround(d2h(c, c.dscal() + 10)));
+      if (k <= 0 || k >= m) continue;
+      // subspace: V = full Q of QR(P * Omega); a second pass with X = P V1 if the split leaks
+      double* Om = c.buf("eig_om", static_cast<size_t>(ldm) * k);
+      ck(fill_random(m, k, Om, ldm, 0x5EEDull + ni * 7919ull + a, c.stream()));
+      gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{Om, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
+      basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
+      const double tol = 10.0 * eps * std::sqrt(static_cast<double>(m)) * std::max(hnorm, 1e-300);
+      double off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
+      S.subspace_passes++;
+      for (int pass = 1; pass < 3 && off > tol; ++pass) {
+        gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{nd.V, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
+        basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
+        off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
+        S.subspace_passes++;
+      }
+      S.max_split_residual = std::max(S.max_split_residual, off / std::max(hnorm, 1e-300));
+      nd.k = k;
+      Node L, R;
+      L.n = k;
+      L.ld = even(k);
+      L.H = mem.alloc(static_cast<size_t>(L.ld) * k);
+      ck(scale_copy(k, k, 1.0, E, ldm, 0, L.H, L.ld, 0, 1, 0.0, c.stream()));
+      ck(symmetrize(k, L.H, L.ld, c.stream()));
+      R.n = m - k;
+      R.ld = even(m - k);
+      R.H = mem.alloc(static_cast<size_t>(R.ld) * (m - k));
+      ck(scale_copy(m - k, m - k, 1.0, E + k + static_cast<int64_t>(k) * ldm, ldm, 0, R.H, R.ld, 0, 1, 0.0,
+                    c.stream()));
+      ck(symmetrize(m - k, R.H, R.ld, c.stream()));
+      nd.left = static_cast<int>(nodes.size());
+      nd.right = nd.left + 1;
+      nodes[ni] = nd;
+      nodes.push_back(L);
+      nodes.push_back(R);
+      S.splits++;
+      ok = true;
+    }
+    if (!ok) return 2;  // no usable split point (all candidates failed)
+    if (ni != 0) mem.release(nodes[ni].H);
+  }
+
+  // ---- leaves: one batched Jacobi launch ----
+  std::vector<JacobiLeaf> leaves;
+  for (auto& nd : nodes)
+    if (nd.leaf) leaves.push_back(JacobiLeaf{nd.H, nd.ld, nd.n, nd.w, nd.Z, even(nd.n)});
+  S.leaves = static_cast<int>(leaves.size());
+  {
+    void* dl = nullptr;
+    ck(cudaMalloc(&dl, sizeof(JacobiLeaf) * leaves.size()));
+    mem.ptrs.push_back(dl);
+    int* dsw = c.ibuf("eig_sweeps", leaves.size());
+    ck(cudaMemcpyAsync(dl, leaves.data(), sizeof(JacobiLeaf) * leaves.size(), cudaMemcpyHostToDevice, c.stream()));
+    ck(jacobi_leaves(static_cast<JacobiLeaf*>(dl), static_cast<int>(leaves.size()), 30, dsw, c.stream()));
+    std::vector<int> sw(leaves.size());
+    ck(cudaMemcpyAsync(sw.data(), dsw, sizeof(int) * sw.size(), cudaMemcpyDeviceToHost, c.stream()));
+    ck(cudaStreamSynchronize(c.stream()));
+    for (int s : sw) S.max_jacobi_sweeps = std::max(S.max_jacobi_sweeps, s);
+  }
+
+  // ---- bottom-up back-transformation ----
+  for (int ni = static_cast<int>(nodes.size()) - 1; ni >= 0; --ni) {
+    Node& nd = nodes[ni];
+    if (nd.leaf) continue;
+    const Node& L = nodes[nd.left];
+    const Node& R = nodes[nd.right];
+    const int m = nd.n, k = nd.k;
+    const int64_t ldm = even(m);
+    gemm(c, 0, 0, m, k, k, 1.0, Mat{nd.V, ldm, 0}, Mat{L.Z, even(L.n), 0}, 0.0, Mat{nd.Z, ldm, 0}, 1);
+    gemm(c, 0, 0, m, m - k, m - k, 1.0, Mat{nd.V + static_cast<int64_t>(k) * ldm, ldm, 0}, Mat{R.Z, even(R.n), 0},
+         0.0, Mat{nd.Z + static_cast<int64_t>(k) * ldm, ldm, 0}, 1);
+    ck(cudaMemcpyAsync(nd.w, L.w, sizeof(double) * k, cudaMemcpyDeviceToDevice, c.stream()));
+    ck(cudaMemcpyAsync(nd.w + k, R.w, sizeof(double) * (m - k), cudaMemcpyDeviceToDevice, c.stream()));
+    S.flops += 2.0 * m * (static_cast<double>(k) * k + static_cast<double>(m - k) * (m - k));
+  }
+
+  // ---- ascending order (dsyevd / ELPA convention) ----
+  const Node& root = nodes[0];
+  std::vector<double> w(n);
+  ck(cudaMemcpyAsync(w.data(), root.w, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  std::vector<int> perm(n);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return w[a] < w[b]; });
+  std::vector<double> ws(n);
+  for (int i = 0; i < n; ++i) ws[i] = w[perm[i]];
+  int* dperm = c.ibuf("eig_perm", n);
+  ck(cudaMemcpyAsync(dperm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream()));
+  ck(cudaMemcpyAsync(dW, ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c.stream()));
+  ck(gather_columns(n, n, root.Z, even(n), dperm, dZ, ldz, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  return 0;
+}
+
+int zoloeig(Context& c, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, int* rk_out,
+            double* dW, double* dZ, int64_t ldz, double* dVfull, int64_t ldv, double* dE, int64_t lde) {
+  const int64_t ldn = even(n);
+  const double eps = 2.220446049250313e-16;
+  const double tol1 = 10.0 * eps / 2.0;
+  // C = (Q - I)/2: minus the projector onto the eigenvalues below the shift (pqdwhsubit.f90:228-239)
+  double* C = c.buf("ze_c", static_cast<size_t>(ldn) * n);
+  ck(scale_copy(n, n, 0.5, dQ, ldq, 0, C, ldn, 0, 1, -0.5, c.stream()));
+  ck(frob2(n, n, C, ldn, c.dpartial(), c.dscal() + 11, c.stream()));
+  const double alpha = d2h(c, c.dscal() + 11);  // ||C||_F^2 (pqdwhsubit.f90:241-243)
+  const int rk = static_cast<int>(std::lround(alpha));
+  *rk_out = rk;
+  ck(frob2(n, n, dA, lda, c.dpartial(), c.dscal() + 12, c.stream()));
+  const double norma = std::sqrt(d2h(c, c.dscal() + 12));
+  if (rk <= 0 || rk >= n) return rk <= 0 ? 0 : 0;
+  int kk = std::min(rk + 3, n);  // oversampling pp = 3 (pqdwhsubit.f90:225)
+  double* X = c.buf("ze_x", static_cast<size_t>(ldn) * n);
+  double* Y = c.buf("ze_y", static_cast<size_t>(ldn) * n);
+  double* V = dVfull ? dVfull : c.buf("ze_v", static_cast<size_t>(ldn) * n);
+  const int64_t ldvv = dVfull ? ldv : ldn;
+  double* E = dE ? dE : c.buf("ze_e", static_cast<size_t>(ldn) * n);
+  const int64_t ldee = dE ? lde : ldn;
+  ck(fill_random(n, kk, X, ldn, 0xC0FFEEull, c.stream()));
+  for (int it = 1; it <= 2; ++it) {
+    // orthonormal basis of X (n x kk), then X = C * basis, then the full n x n Q of its QR
+    double* tau = c.buf("eig_tau", kk);
+    double* T = c.buf("eig_t", static_cast<size_t>((kk + 31) / 32) * 1024);
+    geqrf(c, n, kk, -1, Mat{X, ldn, 0}, tau, T, 1);
+    orgqr(c, n, kk, -1, Mat{X, ldn, 0}, T, Mat{Y, ldn, 0}, 1, kk);
+    gemm(c, 0, 0, n, kk, n, 1.0, Mat{C, ldn, 0}, Mat{Y, ldn, 0}, 0.0, Mat{X, ldn, 0}, 1);
+    basis_from(c, n, kk, Mat{X, ldn, 0}, V, ldvv);
+    const double off = split_residual(c, n, rk, dA, lda, V, ldvv, E, ldee) / norma;
+    // err is the leading-rows block of the reference (E(1:Rk, Rk+1:N)); E is symmetric here
+    if (off <= 4.0 * tol1 || it == 2) break;
+    ck(scale_copy(n, rk, 1.0, V, ldvv, 0, Y, ldn, 0, 1, 0.0, c.stream()));
+    gemm(c, 0, 0, n, rk, n, 1.0, Mat{C, ldn, 0}, Mat{Y, ldn, 0}, 0.0, Mat{X, ldn, 0}, 1);
+    kk = rk;
+  }
+  // eigenpairs of the leading Rk block (PDSYEVD in ZoloEig.f90:98-99), then V1 * VV1
+  const int64_t ldr = even(rk);
+  double* Er = c.buf("ze_er", static_cast<size_t>(ldr) * rk);
+  double* VV = c.buf("ze_vv", static_cast<size_t>(ldr) * rk);
+  ck(scale_copy(rk, rk, 1.0, E, ldee, 0, Er, ldr, 0, 1, 0.0, c.stream()));
+  ck(symmetrize(rk, Er, ldr, c.stream()));
+  const int info = syev_dc(c, rk, Er, ldr, dW, VV, ldr, nullptr);
+  if (info != 0) return info;
+  gemm(c, 0, 0, n, rk, rk, 1.0, Mat{V, ldvv, 0}, Mat{VV, ldr, 0}, 0.0, Mat{dZ, ldz, 0}, 1);
+  ck(cudaStreamSynchronize(c.stream()));
+  return 0;
+}
+
+int svd(Context& c, int m, int n, const double* dA, int64_t lda, int algo, int rk, double* dU, int64_t ldu,
+        double* dS, double* dV, int64_t ldv, EigStats* es) {
+  if (m < n) return -2;
+  const int64_t ldm = even(m), ldn = even(n);
+  double* Q = c.buf("svd_q", static_cast<size_t>(ldm) * n);
+  double* H = c.buf("svd_h", static_cast<size_t>(ldn) * n);
+  int info;
+  if (algo == 0) {
+    QdwhOpts o;
+    info = qdwh(c, m, n, dA, lda, Q, ldm, H, ldn, o);
+  } else {
+    double alpha, beta;
+    info = bounds(c, m, n, 0.0, dA, lda, BOUNDS_ZOLOPD, &alpha, &beta);
+    if (info == 0) info = zolo_pd(c, 'N', rk, m, n, alpha, beta, dA, lda, Q, ldm, H, ldn);
+  }
+  if (info != 0) return info;
+  const Stats pd = c.stats;
+  info = syev_dc(c, n, H, ldn, dS, dV, ldv, es);
+  if (info != 0) return info;
+  gemm(c, 0, 0, m, n, n, 1.0, Mat{Q, ldm, 0}, Mat{dV, ldv, 0}, 0.0, Mat{dU, ldu, 0}, 1);
+  ck(cudaStreamSynchronize(c.stream()));
+  c.stats = pd;
+  return 0;
+}
+
+}  // namespace zolo

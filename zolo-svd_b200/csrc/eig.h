@@ -1,0 +1,38 @@
+// Symmetric eigensolver (spectral divide-and-conquer with Jacobi leaves),
+// ZoloEig and the SVD assembly.  See eig.cpp.
+#pragma once
+#include <cstdint>
+
+#include "context.h"
+
+namespace zolo {
+
+constexpr int kJacobiLeaf = 64;
+
+struct EigStats {
+  int splits = 0;
+  int leaves = 0;
+  int qdwh_calls = 0;
+  int qdwh_iterations = 0;
+  int subspace_passes = 0;
+  int max_jacobi_sweeps = 0;
+  double max_split_residual = 0.0;  // max ||V2^T H V1||_F / ||H||_F over the splits
+  double flops = 0.0;
+};
+
+// H = Z diag(w) Z^T for symmetric H (n x n); w ascending.  Returns 0 or > 0 on failure.
+int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz, EigStats* es);
+
+// ZoloEig (ZoloEig.f90:78-102 with PQDWHSUBIT, pqdwhsubit.f90:227-312): from the polar
+// factor Q of A - sigma I, the Rk = round(||(Q - I)/2||_F^2) eigenpairs of A below sigma:
+// eigenvalues dW (Rk), eigenvectors dZ (n x Rk); optionally the subspace basis V (n x n)
+// and V^T A V.
+int zoloeig(Context& c, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, int* rk,
+            double* dW, double* dZ, int64_t ldz, double* dVfull, int64_t ldv, double* dE, int64_t lde);
+
+// A = U diag(s) V^T (m >= n) by a polar decomposition (algo 0 = QDWH, 1 = Zolo-PD with rk
+// terms) followed by syev_dc of H; s ascending (the order ZoloCHK1 gets from ELPA).
+int svd(Context& c, int m, int n, const double* dA, int64_t lda, int algo, int rk, double* dU, int64_t ldu,
+        double* dS, double* dV, int64_t ldv, EigStats* es);
+
+}  // namespace zolo

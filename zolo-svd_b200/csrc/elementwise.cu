@@ -197,7 +197,71 @@ __global__ void add_diag_kernel(int n, double* A, int64_t lda, double d) {
     A[i + i * lda] += d;
 }
 
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  // SplitMix64 finaliser (Steele, Lea, Flood 2014)
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void fill_random_kernel(int m, int n, double* X, int64_t ldx, uint64_t seed) {
+  const int64_t total = static_cast<int64_t>(m) * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % m), j = static_cast<int>(e / m);
+    const uint64_t r = mix64(seed * 0x100000001B3ull + static_cast<uint64_t>(e));
+    X[i + j * ldx] = 2.0 * (static_cast<double>(r >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+  }
+}
+
+__global__ void trace_kernel(int n, const double* A, int64_t lda, double* out) {
+  __shared__ double sh[TPB / 32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += A[i + i * lda];
+  s = block_sum<TPB>(s, sh);
+  if (threadIdx.x == 0) out[0] = s;
+}
+
+__global__ void gather_columns_kernel(int m, int n, const double* __restrict__ A, int64_t lda, const int* perm,
+                                      double* B, int64_t ldb) {
+  const int64_t total = static_cast<int64_t>(m) * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % m), j = static_cast<int>(e / m);
+    B[i + j * ldb] = A[i + static_cast<int64_t>(perm[j]) * lda];
+  }
+}
+
+__global__ void get_diag_kernel(int n, const double* A, int64_t lda, double* d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = A[i + i * lda];
+}
+
 }  // namespace
+
+cudaError_t fill_random(int m, int n, double* X, int64_t ldx, uint64_t seed, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return cudaSuccess;
+  fill_random_kernel<<<grid_for(static_cast<int64_t>(m) * n), TPB, 0, st>>>(m, n, X, ldx, seed);
+  return cudaGetLastError();
+}
+
+cudaError_t trace(int n, const double* A, int64_t lda, double* out, cudaStream_t st) {
+  trace_kernel<<<1, TPB, 0, st>>>(n, A, lda, out);
+  return cudaGetLastError();
+}
+
+cudaError_t gather_columns(int m, int n, const double* A, int64_t lda, const int* perm, double* B, int64_t ldb,
+                           cudaStream_t st) {
+  if (m <= 0 || n <= 0) return cudaSuccess;
+  gather_columns_kernel<<<grid_for(static_cast<int64_t>(m) * n), TPB, 0, st>>>(m, n, A, lda, perm, B, ldb);
+  return cudaGetLastError();
+}
+
+cudaError_t get_diag(int n, const double* A, int64_t lda, double* d, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  get_diag_kernel<<<(n + TPB - 1) / TPB, TPB, 0, st>>>(n, A, lda, d);
+  return cudaGetLastError();
+}
 
 cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, int64_t strideS, double* dst,
                        int64_t ldd, int64_t strideD, int batch, double diag_add, cudaStream_t st) {

@@ -98,6 +98,27 @@ cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t stride
 cudaError_t apply_t(int w, int n, const double* T, int64_t strideT, double* P, int64_t ldp,
                     int64_t strideP, int trans, int batch, cudaStream_t st);
 
+// ---- eigen stage (jacobi.cu, elementwise.cu) ----
+struct JacobiLeaf {
+  const double* A;  // n x n symmetric (read)
+  int64_t lda;
+  int n;            // <= 64
+  double* w;        // eigenvalues (unsorted)
+  double* V;        // eigenvectors (n x n, ldv)
+  int64_t ldv;
+};
+// One CTA per leaf (device array of descriptors); sweeps[i] receives the sweep count.
+cudaError_t jacobi_leaves(const JacobiLeaf* d_leaves, int count, int max_sweeps, int* d_sweeps, cudaStream_t st);
+// X(i,j) = uniform(-1,1) from a counter hash of (seed, i, j)
+cudaError_t fill_random(int m, int n, double* X, int64_t ldx, uint64_t seed, cudaStream_t st);
+// out[0] = sum_i A(i,i)
+cudaError_t trace(int n, const double* A, int64_t lda, double* out, cudaStream_t st);
+// B(:, j) = A(:, perm[j])
+cudaError_t gather_columns(int m, int n, const double* A, int64_t lda, const int* perm, double* B, int64_t ldb,
+                           cudaStream_t st);
+// d[i] = A(i,i)
+cudaError_t get_diag(int n, const double* A, int64_t lda, double* d, cudaStream_t st);
+
 int num_sms();
 
 }  // namespace zolo

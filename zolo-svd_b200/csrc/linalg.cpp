@@ -165,19 +165,20 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
   }
 }
 
-void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch) {
+void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq) {
+  if (nq < n) nq = n;
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
   Mat V{c.buf("qr_v2", static_cast<size_t>(ldv) * PW * batch * 2), ldv, ldv * PW};
-  Mat P{c.buf("qr_p", static_cast<size_t>(PW) * n * batch), PW, static_cast<int64_t>(PW) * n};
+  Mat P{c.buf("qr_p", static_cast<size_t>(PW) * nq * batch), PW, static_cast<int64_t>(PW) * nq};
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
-  ck(set_identity(mtot, n, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
+  ck(set_identity(mtot, nq, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
   c.stats.launches++;
   for (int pj = npan - 1; pj >= 0; --pj) {
     const int j = pj * PW;
     const int jb = std::min(PW, n - j);
     const int mp = row_hi(mtot, m_top, j, jb) - j;
-    const int nc = n - j;
+    const int nc = nq - j;
     ck(extract_v(mp, jb, W.at(j, j).p, W.ld, W.stride, V.p, V.ld, V.stride, batch, c.stream()));
     c.stats.launches++;
     gemm(c, 1, 0, jb, nc, mp, 1.0, V, Q.at(j, j), 0.0, P, batch);

@@ -47,7 +47,8 @@ void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv 
 // The next panel is factored on a high-priority side stream while the rest of
 // the trailing matrix is updated (look-ahead of depth 1).
 void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch);
-// Explicit Q (mtot x n) from the reflectors of geqrf (mpdorgqr.f / dorgqr).
-void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch);
+// Explicit Q (mtot x nq, nq >= n; default nq = n) from the n reflectors of geqrf
+// (mpdorgqr.f / dorgqr with N >= K).
+void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq = -1);
 
 }  // namespace zolo
