@@ -76,6 +76,14 @@ int zolo_profile_enable(zolo_handle_t handle, int on);
  * current device (negative when the rows do not fit in shared memory). */
 int zolo_panel_cluster_size(int m, int w);
 int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
+/* Algorithm options of a handle (no reference counterpart).
+ * ZOLO_OPT_SHARED_QR: 1 (default) = Zolo-PD QR iterations factor X = Q_x R_x once and
+ * run the r structured QRs on the 2n x n stacks [R_x; sqrt(c_j) I]; 0 = one QR of the
+ * (m+n) x n stack [X; sqrt(c_j) I] per term, as the reference does (pzolopd1.f90:412,
+ * zoloqr.f90:99-111).
+ * Both give the same iterate up to rounding.  Returns -1 for an unknown option. */
+#define ZOLO_OPT_SHARED_QR 1
+int zolo_set_option(zolo_handle_t handle, int option, int value);
 
 /* ---- host scalar routines (no GPU needed) ---- */
 /* Compute_Coeff (Auxil_Zolo.f90:165-200): coeff[0:2rk] = c_i, coeff[2rk:3rk] = -a_i. */

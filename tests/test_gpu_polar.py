@@ -93,6 +93,39 @@ def test_pzolopd1_branch_sequence_matches_oracle():
     h.close()
 
 
+@pytest.mark.parametrize("m,n,rk", [(64, 64, 8), (97, 97, 3), (200, 130, 5), (301, 300, 8), (700, 257, 2)])
+def test_pzolopd1_shared_qr_matches_per_term_qr(m, n, rk):
+    """The QR iterations with one QR of X shared by the r terms (interleaved
+    2n x n stacks) against one QR per (m+n) x n stack (zoloqr.f90:99-111) and
+    against the oracle: same branch sequence, same iterate to rounding."""
+    import torch
+    kappa = 1e6  # the first step takes the QR form; Q is determined to ~kappa*eps
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a, u, v = zo.make_matrix(n, s, 900 + m + n, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)
+    out = {}
+    for shared in (1, 0):
+        h.set_option(zb.OPT_SHARED_QR, shared)
+        dq = torch.zeros_like(da)
+        dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        zb.pzolopd1_dev(h, "N", rk, m, n, al, be, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n)
+        out[shared] = (zb.device_to_colmajor(dq), zb.device_to_colmajor(dh), h.stats())
+    h.close()
+    (q1, h1, st1), (q0, h0, st0) = out[1], out[0]
+    assert st1["branches"] == st0["branches"] and st1["branches"][0] == "QR"  # first step takes the QR form
+    assert st1["iterations"] == st0["iterations"]
+    check_pd(a, q1, h1, n)
+    # both forms are backward stable; Q itself is determined to ~kappa * eps
+    assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
+    assert np.linalg.norm(q1 - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
+    if m == n:
+        q_o, st_o = zo.pzolopd1("N", rk, a, al, be)
+        assert st1["branches"] == st_o.branches
+        assert np.linalg.norm(q1 - q_o) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
+
+
 def test_zolopd_symmetric_vs_oracle():
     rng = np.random.default_rng(9)
     n = 60

@@ -71,6 +71,7 @@ _SIGS = [
     ("zolo_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("zolo_panel_cluster_size", C.c_int, [C.c_int, C.c_int]),
     ("zolo_profile_read", C.c_int, [C.c_void_p, c_double_p, C.c_int]),
+    ("zolo_set_option", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_mellipke", None, [C.c_double, C.c_double, c_double_p, c_double_p]),
     ("zolo_mellipj", None, [C.c_double, C.c_double, C.c_double, c_double_p, c_double_p, c_double_p]),
@@ -121,6 +122,7 @@ _SIGS = [
                             c_double_p, C.c_int, c_double_p, c_int_p]),
 ]
 
+OPT_SHARED_QR = 1
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
@@ -293,6 +295,13 @@ class Handle:
 
     def release(self):
         lib().zolo_release_workspace(self.ptr)
+
+    def set_option(self, option: int, value: int):
+        """Algorithm option of this handle (OPT_SHARED_QR: 1 = one QR of X shared by the
+        Zolotarev terms, 0 = one QR per stacked term as in zoloqr.f90)."""
+        rc = lib().zolo_set_option(self.ptr, option, value)
+        if rc != 0:
+            raise ZoloError(f"zolo_set_option({option}, {value}) returned {rc}")
 
     def profile(self, on: bool = True):
         lib().zolo_profile_enable(self.ptr, 1 if on else 0)

@@ -220,6 +220,14 @@ int zolo_profile_enable(zolo_handle_t h, int on) {
   });
 }
 
+int zolo_set_option(zolo_handle_t h, int option, int value) {
+  return guarded(h, [&](Context& c) {
+    if (option != ZOLO_OPT_SHARED_QR) return -1;
+    c.zolo_shared_qr = value != 0;
+    return 0;
+  });
+}
+
 int zolo_profile_read(zolo_handle_t h, double* out, int reset) {
   return guarded(h, [&](Context& c) {
     c.prof.collect();

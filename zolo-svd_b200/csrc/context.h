@@ -80,6 +80,9 @@ class Context {
   Stats stats;
   Profiler prof;
   std::mutex mu;
+  // Zolo-PD QR iterations: 1 = one QR of X shared by the r terms (default),
+  // 0 = one QR of the stacked [X; sqrt(c_j) I] per term (mpdgeqrf.f form).
+  int zolo_shared_qr = 1;
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles

@@ -36,7 +36,8 @@ __global__ void scale_copy_kernel(int m, int n, double s, const double* __restri
 }
 
 __global__ void form_stack_kernel(int m, int mpad, int n, const double* __restrict__ X, int64_t ldx, double* W,
-                                  int64_t ldw, int64_t strideW, const double* s_vec, double s_scalar) {
+                                  int64_t ldw, int64_t strideW, const double* s_vec, double s_scalar,
+                                  int x_upper) {
   const int b = blockIdx.y;
   double* Wb = W + b * strideW;
   const double s = s_vec ? s_vec[b] : s_scalar;
@@ -46,7 +47,7 @@ __global__ void form_stack_kernel(int m, int mpad, int n, const double* __restri
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int i = static_cast<int>(e % rows), j = static_cast<int>(e / rows);
     double v;
-    if (i < m) v = X[i + j * ldx];
+    if (i < m) v = (x_upper && i > j) ? 0.0 : X[i + j * ldx];
     else v = (i - mpad == j) ? s : 0.0;
     Wb[i + j * ldw] = v;
   }
@@ -272,11 +273,12 @@ cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, i
 }
 
 cudaError_t form_stack(int m, int mpad, int n, const double* X, int64_t ldx, double* W, int64_t ldw,
-                       int64_t strideW, const double* s_vec, double s_scalar, int batch, cudaStream_t st) {
+                       int64_t strideW, const double* s_vec, double s_scalar, int batch, cudaStream_t st,
+                       int x_upper) {
   if (n <= 0 || batch <= 0) return cudaSuccess;
   if (mpad < m) return cudaErrorInvalidValue;
   form_stack_kernel<<<dim3(grid_for(static_cast<int64_t>(mpad + n) * n), batch), TPB, 0, st>>>(
-      m, mpad, n, X, ldx, W, ldw, strideW, s_vec, s_scalar);
+      m, mpad, n, X, ldx, W, ldw, strideW, s_vec, s_scalar, x_upper);
   return cudaGetLastError();
 }
 

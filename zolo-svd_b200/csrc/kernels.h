@@ -41,9 +41,10 @@ cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, i
                        cudaStream_t st);
 // W = [X; 0; s I]: X (m x n) in rows [0,m), zeros in [m,mpad), s I in rows [mpad, mpad+n)
 // (mpad >= m keeps the identity block at an even row offset), batched over s_vec[b] or s_scalar.
+// x_upper: take only the upper triangle of X (zeros below its diagonal).
 cudaError_t form_stack(int m, int mpad, int n, const double* X, int64_t ldx, double* W, int64_t ldw,
                        int64_t strideW, const double* s_vec, double s_scalar, int batch,
-                       cudaStream_t st);
+                       cudaStream_t st, int x_upper = 0);
 // dst(b) = lower(G) + c_b I (lower triangle + diagonal only), batched.
 cudaError_t shift_lower(int n, const double* G, int64_t ldg, double* W, int64_t ldw,
                         int64_t strideW, const double* c_vec, int batch, cudaStream_t st);
@@ -86,14 +87,18 @@ cudaError_t trtri_blocks(int n, const double* L, int64_t ldl, int64_t strideL, d
 // Factor the m x w panel of each batch entry (w <= 32) in place: V below the
 // diagonal (unit diagonal implied), R on/above it, tau[w], T (w x w upper, ldt = w)
 // of the compact WY form I - V T V^T.  Vexp receives V explicitly (m x w, ldv).
+// Row gap: with split > 0, logical row r >= split of the panel is the physical
+// row r + gap of A (two row segments; Vexp stays in logical rows).
 cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, double* tau,
                      int64_t strideTau, double* T, int64_t strideT, double* Vexp, int64_t ldv,
-                     int64_t strideV, int batch, cudaStream_t st);
+                     int64_t strideV, int batch, cudaStream_t st, int split = 0, int64_t gap = 0);
 // Cluster size the panel kernel uses for an m x w panel (negative: rows stay in global memory).
 int qr_panel_config(int m, int w);
-// Vexp = unit-lower-trapezoidal V taken from A (m x w), batched.
+// Vexp = unit-lower-trapezoidal V taken from A (m x w logical rows, same row gap
+// as qr_panel), batched.
 cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t strideA, double* V,
-                      int64_t ldv, int64_t strideV, int batch, cudaStream_t st);
+                      int64_t ldv, int64_t strideV, int batch, cudaStream_t st, int split = 0,
+                      int64_t gap = 0);
 // P'(b) = T(b)^T * P(b) (trans=1) or T(b) * P(b) (trans=0); T w x w upper (ldt=w), P w x n.
 cudaError_t apply_t(int w, int n, const double* T, int64_t strideT, double* P, int64_t ldp,
                     int64_t strideP, int trans, int batch, cudaStream_t st);

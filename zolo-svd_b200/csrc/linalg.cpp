@@ -112,11 +112,37 @@ void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv 
   trsm_rln(c, m, n1, L, X, Y, batch, D, k0);
 }
 
-static inline int row_hi(int mtot, int m_top, int j, int jb) {
-  return m_top >= 0 ? std::min(mtot, m_top + j + jb) : mtot;
+// Rows of panel j (columns j .. j + jb - 1) in the mtot x n matrix: `mp`
+// logical rows, of which the first `split` start at row j and the rest follow
+// after `gap` skipped rows (gap = 0: one window).
+struct PanelRows {
+  int mp, split;
+  int64_t gap;
+};
+
+static inline PanelRows panel_rows(int mtot, int m_top, bool top_tri, int j, int jb) {
+  const int hi = m_top >= 0 ? std::min(mtot, m_top + j + jb) : mtot;
+  if (!top_tri || m_top < 0 || m_top <= j + jb) return PanelRows{hi - j, hi - j, 0};
+  return PanelRows{jb + (hi - m_top), jb, static_cast<int64_t>(m_top) - j - jb};
 }
 
-void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch) {
+// P = V^T B over the panel rows (B starts at the panel's first row)
+static void panel_vt_b(Context& c, const PanelRows& R, int jb, int ncols, Mat V, Mat B, Mat P, int batch) {
+  gemm(c, 1, 0, jb, ncols, R.split, 1.0, V, B, 0.0, P, batch);
+  if (R.split < R.mp)
+    gemm(c, 1, 0, jb, ncols, R.mp - R.split, 1.0, V.at(R.split, 0), B.at(static_cast<int>(R.split + R.gap), 0),
+         1.0, P, batch);
+}
+
+// B -= V P over the panel rows
+static void panel_b_minus_vp(Context& c, const PanelRows& R, int jb, int ncols, Mat V, Mat P, Mat B, int batch) {
+  gemm(c, 0, 0, R.split, ncols, jb, -1.0, V, P, 1.0, B, batch);
+  if (R.split < R.mp)
+    gemm(c, 0, 0, R.mp - R.split, ncols, jb, -1.0, V.at(R.split, 0), P, 1.0,
+         B.at(static_cast<int>(R.split + R.gap), 0), batch);
+}
+
+void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch, bool top_tri) {
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
   // explicit V of consecutive panels alternates between two buffers (look-ahead)
@@ -128,11 +154,11 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
   auto panel = [&](int pj, cudaStream_t st) {
     const int j = pj * PW;
     const int jb = std::min(PW, n - j);
-    const int mp = row_hi(mtot, m_top, j, jb) - j;
+    const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
     Profiler::Rec rec;
-    if (c.prof.on) c.prof.begin(1, 2.0 * mp * static_cast<double>(jb) * jb * batch, st, &rec);
-    ck(qr_panel(mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + pj * PW * PW, strideT, V[pj & 1].p,
-                V[pj & 1].ld, V[pj & 1].stride, batch, st));
+    if (c.prof.on) c.prof.begin(1, 2.0 * R.mp * static_cast<double>(jb) * jb * batch, st, &rec);
+    ck(qr_panel(R.mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + pj * PW * PW, strideT, V[pj & 1].p,
+                V[pj & 1].ld, V[pj & 1].stride, batch, st, R.split, R.gap));
     if (c.prof.on) c.prof.end(rec, st);
     c.stats.launches++;
   };
@@ -140,24 +166,24 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
   for (int pj = 0; pj < npan; ++pj) {
     const int j = pj * PW;
     const int jb = std::min(PW, n - j);
-    const int mp = row_hi(mtot, m_top, j, jb) - j;
+    const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
     const int nc = n - j - jb;
     if (nc <= 0) break;
     const Mat& Vj = V[pj & 1];
     // P = T^T V^T W_trail
-    gemm(c, 1, 0, jb, nc, mp, 1.0, Vj, W.at(j, j + jb), 0.0, P, batch);
+    panel_vt_b(c, R, jb, nc, Vj, W.at(j, j + jb), P, batch);
     ck(apply_t(jb, nc, T + pj * PW * PW, strideT, P.p, P.ld, P.stride, 1, batch, ms));
     c.stats.launches++;
     // next panel's columns first, then the panel on the side stream overlaps the rest
     const int jb2 = std::min(PW, nc);
-    gemm(c, 0, 0, mp, jb2, jb, -1.0, Vj, P, 1.0, W.at(j, j + jb), batch);
+    panel_b_minus_vp(c, R, jb, jb2, Vj, P, W.at(j, j + jb), batch);
     const bool overlap = nc > jb2;
     if (overlap) {
       ck(cudaEventRecord(c.event(0), ms));
       ck(cudaStreamWaitEvent(ss, c.event(0), 0));
       panel(pj + 1, ss);
       ck(cudaEventRecord(c.event(1), ss));
-      gemm(c, 0, 0, mp, nc - jb2, jb, -1.0, Vj, P.at(0, jb2), 1.0, W.at(j, j + jb + jb2), batch);
+      panel_b_minus_vp(c, R, jb, nc - jb2, Vj, P.at(0, jb2), W.at(j, j + jb + jb2), batch);
       ck(cudaStreamWaitEvent(ms, c.event(1), 0));
     } else {
       panel(pj + 1, ms);
@@ -165,7 +191,7 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
   }
 }
 
-void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq) {
+void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq, bool top_tri) {
   if (nq < n) nq = n;
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
@@ -177,14 +203,14 @@ void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q
   for (int pj = npan - 1; pj >= 0; --pj) {
     const int j = pj * PW;
     const int jb = std::min(PW, n - j);
-    const int mp = row_hi(mtot, m_top, j, jb) - j;
+    const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
     const int nc = nq - j;
-    ck(extract_v(mp, jb, W.at(j, j).p, W.ld, W.stride, V.p, V.ld, V.stride, batch, c.stream()));
+    ck(extract_v(R.mp, jb, W.at(j, j).p, W.ld, W.stride, V.p, V.ld, V.stride, batch, c.stream(), R.split, R.gap));
     c.stats.launches++;
-    gemm(c, 1, 0, jb, nc, mp, 1.0, V, Q.at(j, j), 0.0, P, batch);
+    panel_vt_b(c, R, jb, nc, V, Q.at(j, j), P, batch);
     ck(apply_t(jb, nc, T + pj * PW * PW, strideT, P.p, P.ld, P.stride, 0, batch, c.stream()));
     c.stats.launches++;
-    gemm(c, 0, 0, mp, nc, jb, -1.0, V, P, 1.0, Q.at(j, j), batch);
+    panel_b_minus_vp(c, R, jb, nc, V, P, Q.at(j, j), batch);
   }
 }
 

@@ -43,12 +43,18 @@ void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv 
 // Householder QR (in place, panels of 32) of the mtot x n matrices W.  With
 // `m_top` >= 0 the matrix is the stack [X (m_top rows); D] where D is upper
 // triangular: panel j only touches rows j .. m_top + j + 31 (mpdgeqrf.f).
+// With `top_tri` the top block is upper triangular too (its rows below n are
+// zero): panel j then touches two row segments, j .. j + 31 and
+// m_top .. m_top + j + 31, and the rows between them are skipped (the same
+// arithmetic as the full stack, whose skipped rows are zero in the panel).
+// m_top < 0: dense.
 // tau: n per batch entry; T: ceil(n/32) * 32 * 32 per batch entry.
 // The next panel is factored on a high-priority side stream while the rest of
 // the trailing matrix is updated (look-ahead of depth 1).
-void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch);
+void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch, bool top_tri = false);
 // Explicit Q (mtot x nq, nq >= n; default nq = n) from the n reflectors of geqrf
 // (mpdorgqr.f / dorgqr with N >= K).
-void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq = -1);
+void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq = -1,
+           bool top_tri = false);
 
 }  // namespace zolo

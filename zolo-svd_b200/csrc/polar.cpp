@@ -67,6 +67,48 @@ void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
   gemm(c, 0, 1, m, n, n, 1.0, Qf, Qf.at(mp, 0), 0.0, Z, batch, nullptr, 0, 1);
 }
 
+// One Zolo-PD QR step with the QR of X shared by the r terms.  Each term of
+// the reference's QR form (zoloqr.f90:99-111) is Q1_j Q2_j^T / sqrt(c_j) with
+// [X; sqrt(c_j) I] = [Q1_j; Q2_j] R_j.  With X = Q_x R_x,
+//   [X; sqrt(c_j) I] = diag(Q_x, I) [R_x; sqrt(c_j) I],
+// so Q1_j = Q_x Q1'_j and Q2_j = Q2'_j where [Q1'_j; Q2'_j] is the Q factor of
+// the stack of two upper-triangular n x n matrices.  That stack keeps the
+// reference's row order (R_x on top: its rows are the Householder pivots; an
+// interleaved order loses backward stability of the iteration), and panel j
+// touches only rows j .. j+31 of R_x and rows 0 .. j+31 of sqrt(c_j) I.
+// Result: Z(:, :, 0) = Q_x * sum_j w_j Q1'_j Q2'_j^T / FONE, w_j = hw[j].
+// Flops: QR of X 4mn^2 - 4n^3/3, per term 4n^3/3 (structured QR and Q) + n^3
+// (triangular product), and 2mn^2 for the final product -- against
+// r (4mn^2 + n^3) for r independent (m+n) x n stacks.
+void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx, Mat W, Mat Qf, Mat Z, double* tau,
+                          double* T, const double* d_sqrtc, const double* hw, double fone, int rk) {
+  const int64_t ldn = even(n);
+  Mat Xq{c.buf("zq_x", static_cast<size_t>(ldx) * n), ldx, 0};
+  Mat Qx{c.buf("zq_q", static_cast<size_t>(ldx) * n), ldx, 0};
+  ck(scale_copy(m, n, 1.0, X, ldx, 0, Xq.p, Xq.ld, 0, 1, 0.0, c.stream()));
+  c.stats.launches++;
+  geqrf(c, m, n, -1, Xq, tau, T, 1);
+  orgqr(c, m, n, -1, Xq, T, Qx, 1);
+  // W and Qf hold r stacks of (m + n) x n with m >= n: room for r stacks [R_x; 0; sqrt(c_j) I]
+  // of ldn + n rows (the identity block at the even row offset ldn)
+  const int mt = static_cast<int>(ldn), mtot = mt + n;
+  const int64_t lds = even(mtot);
+  Mat Ws{W.p, lds, lds * n}, Qs{Qf.p, lds, lds * n};
+  ck(form_stack(n, mt, n, Xq.p, Xq.ld, Ws.p, Ws.ld, Ws.stride, d_sqrtc, 0.0, rk, c.stream(), 1));
+  c.stats.launches++;
+  geqrf(c, mtot, n, mt, Ws, tau, T, rk, true);
+  orgqr(c, mtot, n, mt, Ws, T, Qs, rk, -1, true);
+  Mat S{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
+  for (int b = 0; b < rk; ++b) {
+    // S += w_b Q1'_b Q2'_b^T; Q2'_b^T is lower triangular, so k starts at the output column
+    const Mat Qb{Qs.p + b * Qs.stride, lds, 0};
+    gemm(c, 0, 1, n, n, n, hw[b] / fone, Qb, Qb.at(mt, 0), b == 0 ? 0.0 : 1.0, S, 1, nullptr, 0, 1);
+  }
+  gemm(c, 0, 0, m, n, n, 1.0, Qx, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
+  const double dm = m, dn = n;
+  c.stats.flops += 4.0 * dm * dn * dn - 4.0 * dn * dn * dn / 3.0 + rk * (7.0 * dn * dn * dn / 3.0) + 2.0 * dm * dn * dn;
+}
+
 // Z(b) = X W_b^{-1} (left = false) or W_b^{-1} X (left = true, square X), W_b = L_b L_b^T.
 void spd_solve(Context& c, int m, int n, const double* X, int64_t ldx, Mat Lw, DiagInv D, Mat Z, int batch,
                bool left) {
@@ -338,24 +380,36 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
                          rk * (static_cast<double>(n) * n * n / 3.0 + 2.0 * m * static_cast<double>(n) * n);
       }
     }
+    const double fone = zolo_fone(coeff.data(), rk);
+    const double con_next = zolo_next_con(con, coeff.data(), rk, fone);
+    bool shared = false;
     if (use_qr) {
       for (int b = 0; b < rk; ++b) hv[b] = std::sqrt(coeff[2 * b]);
       h2d(c, dvec, hv.data(), rk);
-      ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk, c.stream()));
-      c.stats.launches++;
-      geqrf(c, mp + n, n, mp, W, tau, T, rk);
-      orgqr(c, mp + n, n, mp, W, T, Qf, rk);
-      q1q2t(c, m, mp, n, Qf, Z, rk);
       for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b] / std::sqrt(coeff[2 * b]);
+      shared = c.zolo_shared_qr != 0;
+      if (shared) {
+        zolo_terms_shared_qr(c, m, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk);
+      } else {
+        ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk, c.stream()));
+        c.stats.launches++;
+        geqrf(c, mp + n, n, mp, W, tau, T, rk);
+        orgqr(c, mp + n, n, mp, W, T, Qf, rk);
+        q1q2t(c, m, mp, n, Qf, Z, rk);
+        c.stats.flops += rk * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
+      }
       c.stats.qr_iterations++;
       if (it < 16) c.stats.branch[it] = 1;
-      c.stats.flops += rk * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
     }
-    const double fone = zolo_fone(coeff.data(), rk);
-    const double con_next = zolo_next_con(con, coeff.data(), rk, fone);
-    for (int b = 0; b < rk; ++b) hv[16 + b] /= fone;
-    h2d(c, dvec + 16, hv.data() + 16, rk);
-    ck(combine_update(m, n, X, ldx, Z.p, Z.ld, Z.stride, rk, 1.0 / fone, 0.0, dvec + 16, part, scal, c.stream()));
+    if (shared) {
+      // Z already holds sum_j w_j Q1_j Q2_j^T / FONE
+      ck(combine_update(m, n, X, ldx, Z.p, Z.ld, 0, 1, 1.0 / fone, 1.0, nullptr, part, scal, c.stream()));
+    } else {
+      for (int b = 0; b < rk; ++b) hv[16 + b] /= fone;
+      h2d(c, dvec + 16, hv.data() + 16, rk);
+      ck(combine_update(m, n, X, ldx, Z.p, Z.ld, Z.stride, rk, 1.0 / fone, 0.0, dvec + 16, part, scal,
+                        c.stream()));
+    }
     c.stats.launches += 2;
     err = std::sqrt(d2h(c, scal));
     if (it < 16) {

@@ -43,6 +43,8 @@ struct PanelArgs {
   int m, w, rows_per, rp_ld;  // rp_ld: leading dimension of the shared-memory chunk
   double* A;
   int64_t lda, strideA;
+  int split;    // logical rows >= split live `gap` rows further down in A
+  int64_t gap;
   double* tau;
   int64_t strideTau;
   double* T;
@@ -91,9 +93,11 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
   const int grp = lane & 7;                      // row group: local rows grp, grp+8, ...
   const int rp = p.rp_ld;
 
+  // physical row of A holding logical row r
+  auto prow = [&](int r) -> int64_t { return r + (r >= p.split ? p.gap : 0); };
   auto at = [&](int rl, int c) -> double& {
     if (SMEM) return chunk[c * rp + rl];
-    return A[(r0 + rl) + c * lda];
+    return A[prow(r0 + rl) + c * lda];
   };
   // first local row >= global row `from` that belongs to this thread's group
   auto first_row = [&](int from) {
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
     const int tot = w * nloc;
     for (int e = tid; e < tot; e += QT) {
       const int c = e / nloc, rl = e - c * nloc;
-      chunk[c * rp + rl] = A[(r0 + rl) + c * lda];
+      chunk[c * rp + rl] = A[prow(r0 + rl) + c * lda];
     }
   }
   __syncthreads();
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
     const int tot = w * nloc;
     for (int e = tid; e < tot; e += QT) {
       const int c = e / nloc, rl = e - c * nloc;
-      A[(r0 + rl) + c * lda] = chunk[c * rp + rl];
+      A[prow(r0 + rl) + c * lda] = chunk[c * rp + rl];
     }
   }
   cluster.sync();
@@ -322,14 +326,14 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
 }
 
 __global__ void extract_v_kernel(int m, int w, const double* __restrict__ A, int64_t lda, int64_t strideA,
-                                 double* V, int64_t ldv, int64_t strideV) {
+                                 double* V, int64_t ldv, int64_t strideV, int split, int64_t gap) {
   const double* Ab = A + blockIdx.y * strideA;
   double* Vb = V + blockIdx.y * strideV;
   const int64_t total = static_cast<int64_t>(m) * w;
   for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int i = static_cast<int>(e % m), j = static_cast<int>(e / m);
-    double v = (i > j) ? Ab[i + j * lda] : (i == j ? 1.0 : 0.0);
+    double v = (i > j) ? Ab[i + (i >= split ? gap : 0) + j * lda] : (i == j ? 1.0 : 0.0);
     Vb[i + j * ldv] = v;
   }
 }
@@ -437,9 +441,9 @@ int qr_panel_config(int m, int w) {
 
 cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, double* tau, int64_t strideTau,
                      double* T, int64_t strideT, double* Vexp, int64_t ldv, int64_t strideV, int batch,
-                     cudaStream_t st) {
+                     cudaStream_t st, int split, int64_t gap) {
   if (m <= 0 || w <= 0 || batch <= 0) return cudaSuccess;
-  if (w > QW || m < w) return cudaErrorInvalidValue;
+  if (w > QW || m < w || gap < 0 || (gap > 0 && split < w)) return cudaErrorInvalidValue;
   const int maxcl = max_cluster();
   // smallest cluster whose per-CTA row chunk fits in shared memory, with at most ~512 rows per CTA
   int cl = 1;
@@ -454,6 +458,8 @@ cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, doub
   pa.A = A;
   pa.lda = lda;
   pa.strideA = strideA;
+  pa.split = (split > 0 && gap > 0) ? split : m;
+  pa.gap = gap;
   pa.tau = tau;
   pa.strideTau = strideTau;
   pa.T = T;
@@ -467,10 +473,12 @@ cudaError_t qr_panel(int m, int w, double* A, int64_t lda, int64_t strideA, doub
 }
 
 cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t strideA, double* V, int64_t ldv,
-                      int64_t strideV, int batch, cudaStream_t st) {
+                      int64_t strideV, int batch, cudaStream_t st, int split, int64_t gap) {
   if (m <= 0 || w <= 0 || batch <= 0) return cudaSuccess;
+  if (gap < 0 || (gap > 0 && split < w)) return cudaErrorInvalidValue;
+  if (!(split > 0 && gap > 0)) split = m;
   int blocks = static_cast<int>(std::min<int64_t>((static_cast<int64_t>(m) * w + 255) / 256, 2048));
-  extract_v_kernel<<<dim3(blocks, batch), 256, 0, st>>>(m, w, A, lda, strideA, V, ldv, strideV);
+  extract_v_kernel<<<dim3(blocks, batch), 256, 0, st>>>(m, w, A, lda, strideA, V, ldv, strideV, split, gap);
   return cudaGetLastError();
 }
 
