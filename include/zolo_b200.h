@@ -54,7 +54,12 @@ typedef struct {
   int64_t launches;    /* kernels launched                                */
   double con[16];      /* per iteration: CON (Zolo) or c_k (QDWH)         */
   double err[16];      /* per iteration: ||X_{k+1} - X_k||_F              */
-  int branch[16];      /* per iteration: 1 = QR form, 2 = Cholesky form   */
+  int branch[16];      /* per iteration: 1 = QR form, 2 = Cholesky form,
+                          3 = Newton-Schulz step (ZOLO_OPT_NS_FINISH)      */
+  double flops_executed; /* FP64 flops actually executed (the shared-QR form
+                            does fewer than the canonical count)           */
+  int ns_steps;        /* Newton-Schulz steps that ended the iteration     */
+  int ns_finish;       /* 1 if Newton-Schulz steps ended the iteration     */
 } zolo_stats_t;
 
 /* ---- handles (no reference counterpart: the reference is one MPI job) ---- */
@@ -83,6 +88,15 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * zoloqr.f90:99-111).
  * Both give the same iterate up to rounding.  Returns -1 for an unknown option. */
 #define ZOLO_OPT_SHARED_QR 1
+/* ZOLO_OPT_NS_FINISH: 0 (default) = the reference's stopping rule
+ * (pzolopd1.f90:381-397: iterate until ||X_{k+1} - X_k||_F <= (5 eps)^(1/(2r+1))).
+ * 1 = before each Cholesky-form Zolo-PD iteration, measure e = ||X^T X - I||_F/sqrt(n)
+ * from the Gram matrix that iteration forms anyway; once e <= 5e-3, finish with
+ * FP64 Newton-Schulz steps X <- X (3I - X^T X)/2 instead of further Zolo
+ * iterations (1 to 3 steps, as many as e -> 1.5 e^2 needs to reach 1e-16).  The
+ * polar factor of X is that of A, so the result agrees with the reference rule's
+ * to rounding.  No reference counterpart. */
+#define ZOLO_OPT_NS_FINISH 2
 int zolo_set_option(zolo_handle_t handle, int option, int value);
 
 /* ---- host scalar routines (no GPU needed) ---- */

@@ -126,6 +126,55 @@ def test_pzolopd1_shared_qr_matches_per_term_qr(m, n, rk):
         assert np.linalg.norm(q1 - q_o) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
 
 
+def _pzolopd1_dev_run(h, a, rk, al, be, ns_finish):
+    import torch
+    m, n = a.shape
+    h.set_option(zb.OPT_NS_FINISH, ns_finish)
+    da = zb.colmajor_to_device(a)
+    dq = torch.zeros_like(da)
+    dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    zb.pzolopd1_dev(h, "N", rk, m, n, al, be, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n)
+    h.set_option(zb.OPT_NS_FINISH, 0)
+    return zb.device_to_colmajor(dq), zb.device_to_colmajor(dh), h.stats()
+
+
+@pytest.mark.parametrize("m,n,kappa,rk", [(300, 300, 1e12, 8), (256, 256, 1e16, 8), (200, 200, 1e8, 2),
+                                          (330, 200, 1e12, 4), (129, 129, 1e14, 8), (160, 160, 1e10, 1)])
+def test_ns_finish_matches_reference_rule(m, n, kappa, rk):
+    """Finishing with FP64 Newton-Schulz once ||X^T X - I||_F/sqrt(n) <= 5e-3 gives the
+    reference rule's accuracy (10*n*eps) with no more Zolo iterations; the iterations it
+    does run are the reference rule's."""
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a, _, _ = zo.make_matrix(n, s, 500 + m + n + rk, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)
+    q0, h0, st0 = _pzolopd1_dev_run(h, a, rk, al, be, 0)
+    q1, h1, st1 = _pzolopd1_dev_run(h, a, rk, al, be, 1)
+    h.close()
+    assert st0["ns_finish"] == 0 and st0["ns_steps"] == 0
+    it1 = st1["iterations"]
+    assert it1 <= st0["iterations"]
+    assert st1["branches"][:it1] == st0["branches"][:it1]
+    if st1["ns_finish"]:
+        assert 1 <= st1["ns_steps"] <= 3
+        assert st1["branches"][it1:] == ["NS"] * st1["ns_steps"]
+    else:
+        assert st1["ns_steps"] == 0 and it1 == st0["iterations"]
+    if (n, kappa, rk) == (300, 1e12, 8):
+        assert st1["ns_finish"] == 1 and it1 < st0["iterations"]
+    check_pd(a, q1, h1, n)
+    check_pd(a, q0, h0, n)
+    assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
+
+
+def test_set_option_rejects_unknown():
+    h = zb.Handle(0)
+    with pytest.raises(zb.ZoloError):
+        h.set_option(99, 1)
+    h.close()
+
+
 def test_zolopd_symmetric_vs_oracle():
     rng = np.random.default_rng(9)
     n = 60

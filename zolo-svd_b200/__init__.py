@@ -47,6 +47,9 @@ class Stats(C.Structure):
         ("con", C.c_double * 16),
         ("err", C.c_double * 16),
         ("branch", C.c_int * 16),
+        ("flops_executed", C.c_double),
+        ("ns_steps", C.c_int),
+        ("ns_finish", C.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -56,7 +59,9 @@ class Stats(C.Structure):
                     ms_total=self.ms_total, ms_bounds=self.ms_bounds, ms_iter=self.ms_iter, ms_h=self.ms_h,
                     flops=self.flops, launches=int(self.launches),
                     con=list(self.con[: min(it, 16)]), err=list(self.err[: min(it, 16)]),
-                    branches=["QR" if b == 1 else "CH" for b in self.branch[: min(it, 16)]])
+                    branches=[{1: "QR", 2: "CH", 3: "NS"}.get(b, "?")
+                              for b in self.branch[: min(it + self.ns_steps, 16)]],
+                    flops_executed=self.flops_executed, ns_steps=self.ns_steps, ns_finish=self.ns_finish)
 
 
 # (name, restype, argtypes)
@@ -123,6 +128,7 @@ _SIGS = [
 ]
 
 OPT_SHARED_QR = 1
+OPT_NS_FINISH = 2
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
@@ -297,11 +303,13 @@ class Handle:
         lib().zolo_release_workspace(self.ptr)
 
     def set_option(self, option: int, value: int):
-        """Algorithm option of this handle (OPT_SHARED_QR: 1 = one QR of X shared by the
-        Zolotarev terms, 0 = one QR per stacked term as in zoloqr.f90)."""
+        """Algorithm option of this handle.  OPT_SHARED_QR: 1 (default) = one QR of X
+        shared by the Zolotarev terms, 0 = one QR per stacked term as in zoloqr.f90.
+        OPT_NS_FINISH: 0 (default) = the reference's stopping rule, 1 = finish with FP64
+        Newton-Schulz steps once ||X^T X - I||_F / sqrt(n) <= 5e-3."""
         rc = lib().zolo_set_option(self.ptr, option, value)
         if rc != 0:
-            raise ZoloError(f"zolo_set_option({option}, {value}) returned {rc}")
+            raise ZoloError(f"zolo_set_option({option}, {value})", rc)
 
     def profile(self, on: bool = True):
         lib().zolo_profile_enable(self.ptr, 1 if on else 0)

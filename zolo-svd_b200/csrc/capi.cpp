@@ -222,9 +222,15 @@ int zolo_profile_enable(zolo_handle_t h, int on) {
 
 int zolo_set_option(zolo_handle_t h, int option, int value) {
   return guarded(h, [&](Context& c) {
-    if (option != ZOLO_OPT_SHARED_QR) return -1;
-    c.zolo_shared_qr = value != 0;
-    return 0;
+    if (option == ZOLO_OPT_SHARED_QR) {
+      c.zolo_shared_qr = value != 0;
+      return 0;
+    }
+    if (option == ZOLO_OPT_NS_FINISH) {
+      c.zolo_ns_finish = value != 0;
+      return 0;
+    }
+    return -1;
   });
 }
 
@@ -263,6 +269,9 @@ int zolo_get_stats(zolo_handle_t h, zolo_stats_t* out) {
     out->err[i] = s.err[i];
     out->branch[i] = s.branch[i];
   }
+  out->flops_executed = s.flops + s.flops_exec_delta;
+  out->ns_steps = s.ns_steps;
+  out->ns_finish = s.ns_finish;
   return 0;
 }
 

@@ -23,7 +23,10 @@ struct Stats {
   int64_t launches = 0;
   double con[16] = {0};
   double err[16] = {0};
-  int branch[16] = {0};  // 1 = QR, 2 = Cholesky
+  int branch[16] = {0};  // 1 = QR, 2 = Cholesky, 3 = Newton-Schulz
+  double flops_exec_delta = 0.0;  // executed minus canonical flops (shared-QR form: < 0)
+  int ns_steps = 0;
+  int ns_finish = 0;  // 1 if Newton-Schulz steps ended the iteration
 };
 
 // Optional per-kernel-class timing with CUDA events recorded around launches on
@@ -83,6 +86,8 @@ class Context {
   // Zolo-PD QR iterations: 1 = one QR of X shared by the r terms (default),
   // 0 = one QR of the stacked [X; sqrt(c_j) I] per term (mpdgeqrf.f form).
   int zolo_shared_qr = 1;
+  // Zolo-PD stopping: 0 = reference rule, 1 = Newton-Schulz finish once ||X^T X - I|| is small.
+  int zolo_ns_finish = 0;
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles

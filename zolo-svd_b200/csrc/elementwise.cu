@@ -183,6 +183,29 @@ __global__ void transpose_kernel(int m, int n, const double* __restrict__ A, int
   }
 }
 
+// Newton-Schulz step matrix from the lower triangle of G = X^T X: G <- (3I - G)/2
+// (both triangles written; only when `write`) and partial[block] = sum of (G - I)^2
+// over all entries.
+__global__ void ns_prepare_kernel(int n, double* G, int64_t ldg, int write, double* partial) {
+  __shared__ double sh[TPB / 32];
+  const int64_t total = static_cast<int64_t>(n) * n;
+  double s = 0.0;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n), j = static_cast<int>(e / n);
+    if (i < j) continue;
+    const double g = G[i + j * ldg];
+    const double d = (i == j) ? g - 1.0 : g;
+    s += (i == j) ? d * d : 2.0 * d * d;
+    if (!write) continue;
+    const double v = (i == j) ? 1.5 - 0.5 * g : -0.5 * g;
+    G[i + j * ldg] = v;
+    if (i != j) G[j + i * ldg] = v;
+  }
+  s = block_sum<TPB>(s, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
 __global__ void set_identity_kernel(int m, int n, double* Q, int64_t ldq, int64_t strideQ, double diag) {
   double* Qb = Q + blockIdx.y * strideQ;
   const int64_t total = static_cast<int64_t>(m) * n;
@@ -330,6 +353,15 @@ cudaError_t transpose(int m, int n, const double* A, int64_t lda, double* B, int
   dim3 grid((m + 31) / 32, (n + 31) / 32);
   transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(m, n, A, lda, B, ldb);
   return cudaGetLastError();
+}
+
+cudaError_t ns_prepare(int n, double* G, int64_t ldg, double* partial, double* err2, int write, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = static_cast<int>(std::min<int64_t>(grid_for(static_cast<int64_t>(n) * n), 1024));
+  ns_prepare_kernel<<<blocks, TPB, 0, st>>>(n, G, ldg, write, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return reduce_sum(partial, blocks, err2, st);
 }
 
 cudaError_t set_identity(int m, int n, double* Q, int64_t ldq, int64_t strideQ, int batch, double diag,

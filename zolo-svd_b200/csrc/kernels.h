@@ -65,6 +65,10 @@ cudaError_t symmetrize(int n, double* B, int64_t ldb, cudaStream_t st);
 cudaError_t transpose(int m, int n, const double* A, int64_t lda, double* B, int64_t ldb,
                       cudaStream_t st);
 // Q = [I; 0] (m x n, batched)
+// Newton-Schulz step matrix: with `write`, G (lower triangle of X^T X on entry) <-
+// (3I - G)/2, both triangles; always *err2 = ||G_in - I||_F^2 (partial: >= 1024
+// doubles of scratch).
+cudaError_t ns_prepare(int n, double* G, int64_t ldg, double* partial, double* err2, int write, cudaStream_t st);
 cudaError_t set_identity(int m, int n, double* Q, int64_t ldq, int64_t strideQ, int batch,
                          double diag, cudaStream_t st);
 // A(i,i) += d

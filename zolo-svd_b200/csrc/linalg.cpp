@@ -46,7 +46,15 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   cudaStream_t s = st ? st : c.stream();
   Profiler::Rec rec;
   const int cls = tri ? 6 : (M <= 32 ? 3 : (N <= 64 ? 4 : (K <= 64 ? 5 : 0)));
-  if (c.prof.on) c.prof.begin(cls, (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K * batch, s, &rec);
+  if (c.prof.on) {
+    // algorithmic flops: lower triangle only (tri); k >= output column (kfrom_n)
+    double f = (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K;
+    if (kfrom_n) {
+      const double nn = std::min(N, K);
+      f = 2.0 * M * (static_cast<double>(N) * K - nn * (nn - 1.0) / 2.0 - (N - nn) * static_cast<double>(K));
+    }
+    c.prof.begin(cls, f * batch, s, &rec);
+  }
   ck(dgemm(a, c.splitk(), s));
   if (c.prof.on) c.prof.end(rec, s);
   c.stats.launches += need ? 2 : 1;

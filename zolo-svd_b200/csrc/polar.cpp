@@ -106,7 +106,42 @@ void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx
   }
   gemm(c, 0, 0, m, n, n, 1.0, Qx, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
   const double dm = m, dn = n;
-  c.stats.flops += 4.0 * dm * dn * dn - 4.0 * dn * dn * dn / 3.0 + rk * (7.0 * dn * dn * dn / 3.0) + 2.0 * dm * dn * dn;
+  const double executed =
+      4.0 * dm * dn * dn - 4.0 * dn * dn * dn / 3.0 + rk * (7.0 * dn * dn * dn / 3.0) + 2.0 * dm * dn * dn;
+  c.stats.flops_exec_delta += executed - rk * (4.0 * dm * dn * dn + dn * dn * dn);
+}
+
+// Finish of the polar iteration by FP64 Newton-Schulz steps X <- X (3I - X^T X)/2
+// (quadratic: e -> 1.5 e^2 for e = ||X^T X - I||_F / sqrt(n)).  On entry G holds
+// the lower triangle of X^T X and e0 its measured e; the number of steps is the
+// smallest that takes the predicted e below 1e-16 (at most 3 for e0 <= 5e-3).
+// Records the steps as branch 3 after the `it` Zolo iterations.
+void newton_schulz_finish(Context& c, int m, int n, double* X, int64_t ldx, Mat G, Mat Z, double e0, int it) {
+  int steps = 1;
+  for (double e = 1.5 * e0 * e0; e > 1e-16 && steps < 3; e = 1.5 * e * e) ++steps;
+  double* scal = c.dscal();
+  double ek = e0;
+  for (int k = 0; k < steps; ++k) {
+    if (k > 0) {
+      gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+      c.stats.flops += static_cast<double>(m) * n * n;
+    }
+    ck(ns_prepare(n, G.p, G.ld, c.dpartial(), scal + 2, 1, c.stream()));
+    if (k > 0) ek = std::sqrt(d2h(c, scal + 2) / n);
+    gemm(c, 0, 0, m, n, n, 1.0, Mat{X, ldx, 0}, G, 0.0, Mat{Z.p, Z.ld, 0}, 1);
+    ck(scale_copy(m, n, 1.0, Z.p, Z.ld, 0, X, ldx, 0, 1, 0.0, c.stream()));
+    c.stats.launches += 3;
+    c.stats.flops += 2.0 * m * static_cast<double>(n) * n;
+    const int slot = it + c.stats.ns_steps;
+    if (slot < 16) {
+      c.stats.branch[slot] = 3;
+      c.stats.con[slot] = 1.0;
+      c.stats.err[slot] = ek;
+    }
+    c.stats.ns_steps++;
+  }
+  // the SYRK of the first step was counted by the Cholesky branch that measured e0
+  c.stats.flops += static_cast<double>(m) * n * n;
 }
 
 // Z(b) = X W_b^{-1} (left = false) or W_b^{-1} X (left = true, square X), W_b = L_b L_b^T.
@@ -353,6 +388,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   std::vector<double> coeff(3 * rk), hv(64, 0.0);
   double con = 1.0 / beta, err = 1.0;
   int it = 0;
+  const bool ns_finish = c.zolo_ns_finish != 0;
   EventTimer ti(c.stream());
   while (err > tol2 && it < maxit) {
     compute_coeff(con, tol, rk, coeff.data());
@@ -361,6 +397,18 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     bool use_qr = (it == 0 || con > 1.0e3) && maxc > 3.0e2;
     if (!use_qr) {
       gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+      if (ns_finish) {
+        // G = X^T X is in hand: when X is already within 5e-3 of orthogonal, the rest of
+        // the iteration is FP64 Newton-Schulz (the polar factor of X is that of A)
+        ck(ns_prepare(n, G.p, G.ld, part, scal + 2, 0, c.stream()));
+        c.stats.launches += 2;
+        const double e0 = std::sqrt(d2h(c, scal + 2) / n);
+        if (e0 <= 5e-3) {
+          newton_schulz_finish(c, m, n, X, ldx, G, Z, e0, it);
+          c.stats.ns_finish = 1;
+          break;
+        }
+      }
       for (int b = 0; b < rk; ++b) hv[b] = coeff[2 * b];
       h2d(c, dvec, hv.data(), rk);
       ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk, c.stream()));
@@ -396,8 +444,10 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         geqrf(c, mp + n, n, mp, W, tau, T, rk);
         orgqr(c, mp + n, n, mp, W, T, Qf, rk);
         q1q2t(c, m, mp, n, Qf, Z, rk);
-        c.stats.flops += rk * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
       }
+      // canonical: the reference's structured QR form, 4mn^2 + n^3 per term (the shared form
+      // records what it executes beyond this in flops_exec_delta)
+      c.stats.flops += rk * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
       c.stats.qr_iterations++;
       if (it < 16) c.stats.branch[it] = 1;
     }
