@@ -220,9 +220,10 @@ FORMS = {
     "reference_steps": {"shared_qr": 0, "ns_finish": 0},
 }
 
-# DRAM bytes of one launch of the dominant kernel (DMMA GEMM, 128x128 tiles, general shape)
-# from an ncu capture of that kernel; None until a capture is recorded.
-DGEMM_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) of one launch of the dominant kernel (DMMA GEMM, 128x128 tiles)
+# from an ncu capture of a C = A B launch with M = N = K = 4096: 880.5 MB + 120.3 MB.
+DGEMM_TRAFFIC_BYTES = 1.0008e9
+DGEMM_TRAFFIC_LAUNCH = "one 4096^3 C = A B launch (ncu capture; algorithmic A+B+C = 0.40 GB)"
 
 
 def accuracy(torch, dA, dQ, dH, s_true=None) -> dict:
@@ -392,7 +393,7 @@ def run_gpu(args):
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)",
-                         "traffic": DGEMM_TRAFFIC_BYTES,
+                         "traffic": DGEMM_TRAFFIC_BYTES, "traffic_launch": DGEMM_TRAFFIC_LAUNCH,
                          "share_of_step": g["ms"] / prof_ms if prof_ms else None,
                          "launches_per_step": g["launches"]},
             "kernel_classes": per_class,

@@ -1,0 +1,126 @@
+#!/usr/bin/env python
+"""Single-kernel cases of the polar-decomposition path, run through the C-ABI.
+
+Each case builds its operands on the GPU, runs the named operation `--reps`
+times and prints the device time per repetition (CUDA events on the handle's
+stream).  The cases are the shapes that dominate a Zolo-PD / QDWH solve, so a
+profiler pointed at one case sees the same kernel configuration as the full
+solve (e.g. ``ncu -k regex:dgemm_kernel ... python kernel_cases.py --case gemm_nn``):
+
+  gemm_nn      C = A B, M = N = K = n          (general DMMA GEMM, 128 x 128 tiles)
+  gemm_rank32  C -= A B, M = N = n, K = 32     (Householder trailing update, 64 x 64 tiles)
+  gemm_m32     P = V^T W, M = 32, N = K = n    (panel projection, 32 x 64 tiles)
+  syrk         lower(C) = A^T A, n x n          (Gram of the Cholesky form)
+  geqrf        Householder QR of an n x n matrix (panel kernel + trailing GEMMs)
+  potrf        Cholesky of an SPD n x n matrix  (leaf kernel + GEMMs)
+
+  python kernel_cases.py --case gemm_nn --n 4096 --reps 3
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_pkg():
+    if "zolo_svd_b200" in sys.modules:
+        return sys.modules["zolo_svd_b200"]
+    spec = importlib.util.spec_from_file_location("zolo_svd_b200", os.path.join(HERE, "__init__.py"),
+                                                  submodule_search_locations=[HERE])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["zolo_svd_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+CASES = ("gemm_nn", "gemm_rank32", "gemm_m32", "syrk", "geqrf", "potrf")
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", choices=CASES, required=True)
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    import torch
+    zb = load_pkg()
+    n = args.n
+    h = zb.Handle(0)
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    f64 = dict(dtype=torch.float64, device="cuda")
+
+    def randn(r, c):
+        return torch.randn(c, r, generator=g, **f64)  # column-major r x c (torch row-major c x r)
+
+    lib = zb.lib()
+    flops = 0.0
+    if args.case in ("gemm_nn", "gemm_rank32", "gemm_m32", "syrk"):
+        if args.case == "gemm_nn":
+            M, N, K, ta, tri = n, n, n, b"N", 0
+        elif args.case == "gemm_rank32":
+            M, N, K, ta, tri = n, n, 32, b"N", 0
+        elif args.case == "gemm_m32":
+            M, N, K, ta, tri = 32, n, n, b"T", 0
+        else:
+            M, N, K, ta, tri = n, n, n, b"T", 1
+        a = randn(K, M) if ta == b"T" else randn(M, K)
+        b = randn(K, N)
+        c = randn(M, N)
+        lda = a.shape[1]
+        beta = -1.0 if args.case == "gemm_rank32" else 0.0
+        alpha = -1.0 if args.case == "gemm_rank32" else 1.0
+        flops = (1.0 if tri else 2.0) * M * N * K
+
+        def run():
+            rc = lib.zolo_dgemm_dev(h.ptr, ta, b"N", M, N, K, alpha, a.data_ptr(), lda, b.data_ptr(), K, beta,
+                                    c.data_ptr(), M, tri, 0)
+            if rc:
+                raise zb.ZoloError("zolo_dgemm_dev", rc)
+    elif args.case == "geqrf":
+        w0 = randn(n, n)
+        w = torch.empty_like(w0)
+        tau = torch.empty(n, **f64)
+        t = torch.empty(((n + 31) // 32) * 1024, **f64)
+        flops = 4.0 / 3.0 * n ** 3
+
+        def run():
+            w.copy_(w0)
+            rc = lib.zolo_dgeqrf_dev(h.ptr, n, n, -1, w.data_ptr(), n, tau.data_ptr(), t.data_ptr())
+            if rc:
+                raise zb.ZoloError("zolo_dgeqrf_dev", rc)
+    else:
+        x = randn(n, n)
+        spd = (x.T @ x) / n + torch.eye(n, **f64)
+        w = torch.empty_like(spd)
+        flops = n ** 3 / 3.0
+
+        def run():
+            w.copy_(spd)
+            rc = lib.zolo_dpotrf_dev(h.ptr, n, w.data_ptr(), n)
+            if rc:
+                raise zb.ZoloError("zolo_dpotrf_dev", rc)
+
+    run()
+    torch.cuda.synchronize()
+    for i in range(args.reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(f"{args.case} n={n} rep {i}: {ms:.3f} ms, {flops / (ms * 1e-3) / 1e12:.2f} TFLOP/s", flush=True)
+    h.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
