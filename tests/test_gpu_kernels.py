@@ -70,6 +70,44 @@ def test_dgemm_vs_numpy(h, ta, tb, mnk):
     assert np.all(np.abs(host(dc) - ref) <= bound + 1e-300)
 
 
+# rank-k updates C = beta*C + alpha*A*B with K <= 32 and M*N >= 16 * 128 * 32 take the
+# persistent streaming kernel (update.cu): partial tiles, K < 8, odd M and K with
+# 16-byte copies (even leading dimensions), odd leading dimensions and 8-byte-aligned
+# (not 16) pointers (8-byte copies), beta = 0 (C not read) and beta = 1
+@pytest.mark.parametrize("m,n,k,alpha,beta,off,pad", [
+    (512, 512, 32, -1.0, 1.0, 0, 0), (1000, 700, 7, 0.5, 1.0, 1, 1), (300, 1200, 1, -1.0, 1.0, 0, 0),
+    (129, 2049, 31, 1.0, 0.0, 1, 2), (4100, 70, 32, -1.0, 1.0, 0, 0), (777, 333, 16, 2.0, -0.5, 1, 1),
+    (1001, 300, 31, -1.0, 1.0, 0, 1), (255, 1031, 17, -1.0, 1.0, 0, 1), (1026, 1000, 16, 1.5, 0.0, 0, 0),
+    (2050, 520, 2, -1.0, 1.0, 0, 2)])
+def test_dgemm_streaming_rank_update(h, m, n, k, alpha, beta, off, pad):
+    import torch
+    rng = np.random.default_rng(m + n + k)
+    a = rng.standard_normal((m, k))
+    b = rng.standard_normal((k, n))
+    c0 = rng.standard_normal((m, n))
+    lda, ldb, ldc = m + pad, k + pad, m + pad
+    def padded(x, ld):
+        buf = torch.zeros(x.shape[1] * ld + off, dtype=torch.float64, device="cuda")
+        view = buf[off:off + x.shape[1] * ld].view(x.shape[1], ld)
+        view[:, : x.shape[0]] = torch.from_numpy(np.ascontiguousarray(x.T)).cuda()
+        return buf, view
+    ba, va = padded(a, lda)
+    bb, vb = padded(b, ldb)
+    bc, vc = padded(c0, ldc)
+    torch.cuda.synchronize()
+    r = zb.lib().zolo_dgemm_dev(h.ptr, b"N", b"N", m, n, k, alpha, va.data_ptr(), lda, vb.data_ptr(), ldb, beta,
+                                vc.data_ptr(), ldc, 0, 0)
+    assert r == 0
+    torch.cuda.synchronize()
+    got = vc[:, :m].T.cpu().numpy()
+    ref = alpha * a @ b + beta * c0
+    bound = 2 * (k + 2) * EPS * (abs(alpha) * np.abs(a) @ np.abs(b) + abs(beta) * np.abs(c0))
+    assert np.all(np.abs(got - ref) <= bound + 1e-300)
+    # the padding rows of C (ldc > m) are untouched
+    if pad:
+        assert torch.count_nonzero(vc[:, m:]).item() == 0
+
+
 def test_dgemm_lower_triangle_only(h):
     rng = np.random.default_rng(1)
     m, k = 300, 77

@@ -93,7 +93,7 @@ def test_pzolopd1_branch_sequence_matches_oracle():
     h.close()
 
 
-@pytest.mark.parametrize("m,n,rk", [(64, 64, 8), (97, 97, 3), (200, 130, 5), (301, 300, 8), (700, 257, 2)])
+@pytest.mark.parametrize("m,n,rk", [(64, 64, 8), (97, 97, 3), (200, 130, 5), (301, 300, 8), (700, 257, 2), (600, 600, 4)])
 def test_pzolopd1_shared_qr_matches_per_term_qr(m, n, rk):
     """The QR iterations with one QR of X shared by the r terms (interleaved
     2n x n stacks) against one QR per (m+n) x n stack (zoloqr.f90:99-111) and

@@ -427,6 +427,7 @@ cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
   if (!al8(a.A) || !al8(a.B) || !al8(a.C)) return cudaErrorMisalignedAddress;
   const bool v16 = al(a.A, a.lda) && al(a.B, a.ldb) && al(a.C, a.ldc) &&
                    (a.batch <= 1 || ((a.strideA | a.strideB | a.strideC) & 1) == 0);
+  if (rank_update_applies(a)) return rank_update(a, st);
   const int sms = num_sms();
   if (a.K <= 0) {
     // C = beta*C

@@ -33,6 +33,10 @@ struct Scratch {
 
 cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st);
 size_t dgemm_splitk_bytes(const GemmArgs& a, int num_sms);
+// Streaming rank-k update C = beta*C + alpha*A*B (no transposes, K <= 32; update.cu).
+// dgemm dispatches to it when rank_update_applies(a).
+bool rank_update_applies(const GemmArgs& a);
+cudaError_t rank_update(const GemmArgs& a, cudaStream_t st);
 
 // ---- elementwise / reductions (elementwise.cu) ----
 // dst(i,j) = s * src(i,j) (+ d on the diagonal), batched.
