@@ -19,7 +19,11 @@
  * GPU failures are reported as INFO = -1000 - cudaError_t.  Nothing aborts.
  *
  * Threading: every handle owns one CUDA stream; calls on one handle are
- * serialised by a mutex.  The reference-named host-array entry points use a
+ * serialised by a mutex.  The handle's own stream is a blocking stream, so a
+ * call is ordered after work already queued on the legacy default stream; with
+ * zolo_set_stream the caller's stream is used instead and the caller orders the
+ * inputs on it.  The device-pointer solvers return after their results are
+ * complete.  The reference-named host-array entry points use a
  * process-wide default handle on device 0 (or ZOLO_DEVICE).
  */
 #ifndef ZOLO_B200_H

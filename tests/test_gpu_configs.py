@@ -1,0 +1,121 @@
+"""The reference's workloads at full size on the GPU, through the device entry
+points, checked by size-independent properties against the prescribed singular
+values (the polar factor U V^T and H = V diag(s) V^T are known by construction):
+
+  QDWH-PD, n = 1024, kappa = 1e8                          (PQDWHFACS path)
+  Zolo-PD r = 8, n = 4096, kappa = 1e16, 5 % duplicated sigma (PZOLOPD1 path)
+  Zolo-SVD, 16384 x 8192, kappa = 1e10: 70 % of sigma geometric, 20 % exactly 1,
+  10 % in clusters of relative gap 1e-9                   (ZoloCHK1 assembly)
+
+Inputs are seeded synthetic matrices with the workloads' shapes and spectra,
+generated on the GPU.  Tolerances: backward error / residual and orthogonality
+<= 10*n*eps, singular values within 1e-12 of sigma_max."""
+import math
+
+import numpy as np
+import pytest
+
+import zolo_svd_b200 as zb
+from oracle import zolo_oracle as zo
+
+pytestmark = pytest.mark.gpu
+EPS = zo.EPS
+
+
+def _haar(torch, m, n, g):
+    q, r = torch.linalg.qr(torch.randn(m, n, dtype=torch.float64, device="cuda", generator=g))
+    return q * torch.sign(torch.diagonal(r))[None, :]
+
+
+def _orth(torch, q):
+    n = q.shape[1]
+    return float(torch.linalg.norm(q.T @ q - torch.eye(n, dtype=torch.float64, device="cuda")) / math.sqrt(n))
+
+
+@pytest.fixture(scope="module")
+def h():
+    hd = zb.Handle(0)
+    yield hd
+    hd.close()
+
+
+def test_qdwh_n1024_kappa1e8(h):
+    import torch
+    n = 1024
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1001)
+    s = torch.logspace(0, -8, n, dtype=torch.float64, device="cuda")
+    u, v = _haar(torch, n, n, g), _haar(torch, n, n, g)
+    a = (u * s[None, :]) @ v.T  # row-major view of A
+    da = a.T.contiguous()  # column-major storage
+    dq, dh = torch.empty_like(da), torch.empty_like(da)
+    zb.qdwh_dev(h, "N", n, n, 0.0, da.data_ptr(), n, dq.data_ptr(), n, dh.data_ptr(), n, 0, 12, 0)
+    q, hh = dq.T, dh.T
+    assert float(torch.linalg.norm(a - q @ hh) / torch.linalg.norm(a)) <= 10 * n * EPS
+    assert _orth(torch, q) <= 10 * n * EPS
+    # the polar factor is determined to ~kappa * eps
+    assert float(torch.linalg.norm(q - u @ v.T)) / math.sqrt(n) <= 100 * n * EPS * 1e8
+    ev = torch.sort(torch.linalg.eigvalsh(0.5 * (hh + hh.T)), descending=True).values
+    assert float(torch.max(torch.abs(ev - s))) <= 1e-12
+
+
+@pytest.mark.parametrize("ns_finish", [0, 1])
+def test_zolopd_n4096_kappa1e16_clusters(h, ns_finish):
+    import torch
+    n = 4096
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1002)
+    s = torch.logspace(0, -16, n, dtype=torch.float64, device="cuda")
+    idx = torch.randperm(n - 1, generator=g, device="cuda")[: n // 20] + 1
+    s[idx] = s[idx - 1]  # 5 % of the values duplicated from a neighbour
+    s = torch.sort(s, descending=True).values
+    u, v = _haar(torch, n, n, g), _haar(torch, n, n, g)
+    a = (u * s[None, :]) @ v.T
+    da = a.T.contiguous()
+    dq, dh = torch.empty_like(da), torch.empty_like(da)
+    h.set_option(zb.OPT_NS_FINISH, ns_finish)
+    try:
+        al, be, info = zb.bounds_dev(h, n, n, da.data_ptr(), n, mode=1)
+        assert info == 0
+        zb.pzolopd1_dev(h, "N", 8, n, n, al, be, da.data_ptr(), n, dq.data_ptr(), n, dh.data_ptr(), n)
+        st = h.stats()
+    finally:
+        h.set_option(zb.OPT_NS_FINISH, 0)
+    assert st["branches"][0] == "QR"
+    q, hh = dq.T, dh.T
+    assert float(torch.linalg.norm(a - q @ hh) / torch.linalg.norm(a)) <= 10 * n * EPS
+    assert _orth(torch, q) <= 10 * n * EPS
+    ev = torch.sort(torch.linalg.eigvalsh(0.5 * (hh + hh.T)), descending=True).values
+    assert float(torch.max(torch.abs(ev - s))) <= 1e-12
+
+
+def test_zolo_svd_16384x8192_clustered(h):
+    import torch
+    m, n = 16384, 8192
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1005)
+    n70, n20 = int(0.7 * n), int(0.2 * n)
+    n10 = n - n70 - n20
+    geo = torch.logspace(0, -10, n70, dtype=torch.float64, device="cuda")
+    one = torch.ones(n20, dtype=torch.float64, device="cuda")
+    base = torch.logspace(-1, -9, n10 // 8 + 1, dtype=torch.float64, device="cuda")
+    rel = 1 + 1e-9 * torch.arange(8, dtype=torch.float64, device="cuda")
+    clusters = (base[:, None] * rel[None, :]).reshape(-1)[:n10]
+    s = torch.sort(torch.cat([geo, one, clusters]), descending=True).values
+    u, v = _haar(torch, m, n, g), _haar(torch, n, n, g)
+    a = (u * s[None, :]) @ v.T  # row-major view of the m x n matrix
+    del u, v
+    da = a.T.contiguous()
+    du = torch.empty_like(da)
+    ds = torch.empty(n, dtype=torch.float64, device="cuda")
+    dv = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    zb.svd_dev(h, m, n, da.data_ptr(), m, du.data_ptr(), m, ds.data_ptr(), dv.data_ptr(), n, algo=1, rk=8)
+    U, V = du.T, dv.T
+    assert float(torch.linalg.norm(a - (U * ds[None, :]) @ V.T) / torch.linalg.norm(a)) <= 10 * n * EPS
+    assert float(torch.max(torch.abs(torch.sort(ds, descending=True).values - s))) <= 1e-12 * float(s[0])
+    assert _orth(torch, U) <= 10 * n * EPS
+    assert _orth(torch, V) <= 10 * n * EPS
+    assert bool(torch.all(ds[1:] >= ds[:-1]))  # ascending, as ELPA returns them
+    del a, da, du, dv
+    torch.cuda.empty_cache()
+    h.release()

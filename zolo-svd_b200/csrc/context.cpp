@@ -4,11 +4,15 @@ namespace zolo {
 
 Context::Context(int device) : device_(device) {
   ck(cudaSetDevice(device));
-  ck(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+  // Blocking streams: work on them is ordered after work already queued on the
+  // legacy default stream (where a caller typically produced the inputs), as on a
+  // cuBLAS handle's default stream.  A non-blocking stream would let a solve read
+  // its input before the producing kernel on the default stream has finished.
+  ck(cudaStreamCreateWithFlags(&own_stream_, cudaStreamDefault));
   stream_ = own_stream_;
   int lo = 0, hi = 0;
   ck(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-  ck(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, hi));
+  ck(cudaStreamCreateWithPriority(&side_, cudaStreamDefault, hi));
   for (auto& e : ev_) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
 
