@@ -168,6 +168,29 @@ def test_ns_finish_matches_reference_rule(m, n, kappa, rk):
     assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
 
 
+def test_solves_are_bitwise_reproducible():
+    """Fixed reduction orders everywhere (no floating-point atomics): the same
+    solve twice gives the same bits, for both Zolo-PD forms and QDWH."""
+    import torch
+    n = 300
+    s = np.geomspace(1.0, 1e-12, n)
+    a, _, _ = zo.make_matrix(n, s, 4242)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    outs = []
+    for rep in range(2):
+        dq = torch.zeros_like(da)
+        al, be, _ = zb.bounds_dev(h, n, n, da.data_ptr(), n, mode=1)
+        zb.pzolopd1_dev(h, "N", 8, n, n, al, be, da.data_ptr(), n, dq.data_ptr(), n)
+        dq2 = torch.zeros_like(da)
+        zb.qdwh_dev(h, "N", n, n, 0.0, da.data_ptr(), n, dq2.data_ptr(), n, 0, 1, 0, 12, 0)
+        outs.append((al, be, dq.clone(), dq2.clone()))
+    h.close()
+    assert outs[0][0] == outs[1][0] and outs[0][1] == outs[1][1]
+    assert torch.equal(outs[0][2], outs[1][2])
+    assert torch.equal(outs[0][3], outs[1][3])
+
+
 def test_set_option_rejects_unknown():
     h = zb.Handle(0)
     with pytest.raises(zb.ZoloError):

@@ -276,16 +276,23 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
     }
     for (int e = tid; e < QW * QW; e += QT) S.G[e] = 0.0;
     __syncthreads();
+    // warps add their partials one after another: a fixed summation order, so the
+    // panel (and everything downstream) is bitwise reproducible run to run
+    for (int wq = 0; wq < QT / 32; ++wq) {
+      if (warp == wq) {
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+        for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int bb = 0; bb < 4; ++bb) {
-        const int i = a * 16 + gq, j = bb * 8 + 2 * tq;
-        atomicAdd(&S.G[i + j * QW], accg[a][bb][0]);
-        atomicAdd(&S.G[i + (j + 1) * QW], accg[a][bb][1]);
-        atomicAdd(&S.G[i + 8 + j * QW], accg[a][bb][2]);
-        atomicAdd(&S.G[i + 8 + (j + 1) * QW], accg[a][bb][3]);
+          for (int bb = 0; bb < 4; ++bb) {
+            const int i = a * 16 + gq, j = bb * 8 + 2 * tq;
+            S.G[i + j * QW] += accg[a][bb][0];
+            S.G[i + (j + 1) * QW] += accg[a][bb][1];
+            S.G[i + 8 + j * QW] += accg[a][bb][2];
+            S.G[i + 8 + (j + 1) * QW] += accg[a][bb][3];
+          }
       }
+      __syncthreads();
+    }
   }
   if (SMEM) {
     const int tot = w * nloc;
