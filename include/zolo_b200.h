@@ -169,6 +169,21 @@ void pzolopd2_(const char* sym, const int* rk, const int* m, const int* n, const
  * dH may be NULL.  Returns INFO. */
 int zolo_qdwh_dev(zolo_handle_t h, char sym, int m, int n, double sigma, const double* dA, int64_t lda, double* dQ,
                   int64_t ldq, double* dH, int64_t ldh, int bounds_mode, int maxit, int left_solve);
+/* Batched QDWH-PD of `count` matrices of different sizes on device arrays (no
+ * counterpart in the reference, whose drivers factor one matrix per MPI job): member i
+ * is the m[i] x n[i] matrix dA[i] (m[i] >= n[i]); dQ[i] receives its polar factor and,
+ * when dH is not NULL, dH[i] its H.  Each member follows PQDWHFACS (SYM = 'N',
+ * SIGMA = 0, PQDWHFACS bounds on the padded member); members are grouped into buckets
+ * of one padded size and each bucket runs as one batched solve with per-member
+ * weights and convergence (padding [[A, 0], [0, tau I]] with tau = ||A||_F/sqrt(n)
+ * leaves the polar factor and the condition number unchanged).  The pointer and size
+ * arrays are host arrays.  info[i] = 0, or > 0 when member i's bounds failed (zero or
+ * non-finite input; its outputs are then undefined); iterations[i] (may be NULL)
+ * receives member i's iteration count.  Returns 0, or < 0 for a bad argument / GPU
+ * failure. */
+int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, const double* const* dA,
+                        const int64_t* lda, double* const* dQ, const int64_t* ldq, double* const* dH,
+                        const int64_t* ldh, int* info, int* iterations);
 /* Zolo-PD (PZOLOPD1 semantics) on device arrays; dH may be NULL.  Returns INFO. */
 int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
                       int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh);

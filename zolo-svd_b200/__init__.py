@@ -93,6 +93,9 @@ _SIGS = [
                              C.c_int, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p, C.c_char]),
     ("zolo_pzolopd2", None, [C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, c_double_p, C.c_int,
                              C.c_int, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p, C.c_char]),
+    ("zolo_qdwh_batch_dev", C.c_int, [C.c_void_p, C.c_int, c_int_p, c_int_p, C.POINTER(C.c_void_p),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_void_p), C.POINTER(C.c_int64), c_int_p, c_int_p]),
     ("zolo_qdwh_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64,
                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int]),
     ("zolo_pzolopd1_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -347,6 +350,25 @@ def qdwh_dev(h: Handle, sym: str, m: int, n: int, sigma: float, dA: int, lda: in
              dH: int = 0, ldh: int = 1, bounds_mode: int = 0, maxit: int = 12, left_solve: int = 0) -> int:
     return _ck("zolo_qdwh_dev", lib().zolo_qdwh_dev(h.ptr, sym.encode()[:1], m, n, sigma, dA, lda, dQ, ldq,
                                                    dH or None, ldh, bounds_mode, maxit, left_solve))
+
+
+def qdwh_batch_dev(h: Handle, members, with_h: bool = True):
+    """Batched QDWH-PD on device arrays.  `members` is a list of
+    (m, n, dA, lda, dQ, ldq, dH, ldh) with device pointers (dH may be 0 when
+    with_h is False).  Returns (info list, iterations list)."""
+    k = len(members)
+    m = (C.c_int * k)(*[x[0] for x in members])
+    n = (C.c_int * k)(*[x[1] for x in members])
+    a = (C.c_void_p * k)(*[x[2] for x in members])
+    lda = (C.c_int64 * k)(*[x[3] for x in members])
+    q = (C.c_void_p * k)(*[x[4] for x in members])
+    ldq = (C.c_int64 * k)(*[x[5] for x in members])
+    hh = (C.c_void_p * k)(*[x[6] for x in members]) if with_h else None
+    ldh = (C.c_int64 * k)(*[x[7] for x in members]) if with_h else None
+    info = (C.c_int * k)()
+    its = (C.c_int * k)()
+    _ck("zolo_qdwh_batch_dev", lib().zolo_qdwh_batch_dev(h.ptr, k, m, n, a, lda, q, ldq, hh, ldh, info, its))
+    return list(info), list(its)
 
 
 def pzolopd1_dev(h: Handle, sym: str, rk: int, m: int, n: int, alpha: float, beta: float, dA: int, lda: int,

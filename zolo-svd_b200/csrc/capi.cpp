@@ -361,6 +361,16 @@ int zolo_qdwh_dev(zolo_handle_t h, char sym, int m, int n, double sigma, const d
   });
 }
 
+int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, const double* const* dA,
+                        const int64_t* lda, double* const* dQ, const int64_t* ldq, double* const* dH,
+                        const int64_t* ldh, int* info, int* iterations) {
+  if (count < 0) return -2;
+  if (count > 0 && (!m || !n || !dA || !lda || !dQ || !ldq || !info || (dH && !ldh))) return -3;
+  return guarded(h, [&](Context& c) {
+    return zolo::qdwh_batch(c, count, m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, nullptr);
+  });
+}
+
 int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
                       int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh) {
   return guarded(h, [&](Context& c) {

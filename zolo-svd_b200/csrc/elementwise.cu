@@ -37,8 +37,9 @@ __global__ void scale_copy_kernel(int m, int n, double s, const double* __restri
 
 __global__ void form_stack_kernel(int m, int mpad, int n, const double* __restrict__ X, int64_t ldx, double* W,
                                   int64_t ldw, int64_t strideW, const double* s_vec, double s_scalar,
-                                  int x_upper) {
+                                  int x_upper, int64_t strideX) {
   const int b = blockIdx.y;
+  X += b * strideX;
   double* Wb = W + b * strideW;
   const double s = s_vec ? s_vec[b] : s_scalar;
   const int rows = mpad + n;
@@ -297,11 +298,11 @@ cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, i
 
 cudaError_t form_stack(int m, int mpad, int n, const double* X, int64_t ldx, double* W, int64_t ldw,
                        int64_t strideW, const double* s_vec, double s_scalar, int batch, cudaStream_t st,
-                       int x_upper) {
+                       int x_upper, int64_t strideX) {
   if (n <= 0 || batch <= 0) return cudaSuccess;
   if (mpad < m) return cudaErrorInvalidValue;
   form_stack_kernel<<<dim3(grid_for(static_cast<int64_t>(mpad + n) * n), batch), TPB, 0, st>>>(
-      m, mpad, n, X, ldx, W, ldw, strideW, s_vec, s_scalar, x_upper);
+      m, mpad, n, X, ldx, W, ldw, strideW, s_vec, s_scalar, x_upper, strideX);
   return cudaGetLastError();
 }
 

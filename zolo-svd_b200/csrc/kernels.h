@@ -45,10 +45,11 @@ cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, i
                        cudaStream_t st);
 // W = [X; 0; s I]: X (m x n) in rows [0,m), zeros in [m,mpad), s I in rows [mpad, mpad+n)
 // (mpad >= m keeps the identity block at an even row offset), batched over s_vec[b] or s_scalar.
-// x_upper: take only the upper triangle of X (zeros below its diagonal).
+// x_upper: take only the upper triangle of X (zeros below its diagonal).  strideX: X of
+// batch entry b at X + b*strideX (0: one X shared by the batch, the r Zolotarev terms).
 cudaError_t form_stack(int m, int mpad, int n, const double* X, int64_t ldx, double* W, int64_t ldw,
                        int64_t strideW, const double* s_vec, double s_scalar, int batch,
-                       cudaStream_t st, int x_upper = 0);
+                       cudaStream_t st, int x_upper = 0, int64_t strideX = 0);
 // dst(b) = lower(G) + c_b I (lower triangle + diagonal only), batched.
 cudaError_t shift_lower(int n, const double* G, int64_t ldg, double* W, int64_t ldw,
                         int64_t strideW, const double* c_vec, int batch, cudaStream_t st);
@@ -133,5 +134,42 @@ cudaError_t gather_columns(int m, int n, const double* A, int64_t lda, const int
 cudaError_t get_diag(int n, const double* A, int64_t lda, double* d, cudaStream_t st);
 
 int num_sms();
+
+// ---- batched polar decomposition (batch.cu) ----
+// One matrix of a batch: A (m x n) in, Q (m x n) and H (n x n, may be null) out, and
+// the value tau of the identity block that pads it to the bucket size.
+struct BatchMember {
+  int m, n;
+  const double* A;
+  int64_t lda;
+  double tau;
+  double* Q;
+  int64_t ldq;
+  double* H;
+  int64_t ldh;
+};
+// P(b) = [[A_b, 0], [0, tau_b I], [0, 0]] (MB x NB)
+cudaError_t batch_pack(const BatchMember* d_mem, int count, int MB, int NB, double* P, int64_t ldp, int64_t sp,
+                       cudaStream_t st);
+// Q_b = Q'(b)[0:m, 0:n], H_b = H'(b)[0:n, 0:n]
+cudaError_t batch_unpack(const BatchMember* d_mem, int count, int MB, int NB, const double* Q, int64_t ldq,
+                         int64_t sq, const double* H, int64_t ldh, int64_t sh, cudaStream_t st);
+// out[b] = ||X_b||_F^2 (partial: partial_cap doubles of scratch)
+cudaError_t batch_frob2(int m, int n, const double* X, int64_t ldx, int64_t sx, int batch, double* partial,
+                        int partial_cap, double* out, cudaStream_t st);
+// out[b] = ||X_b||_1 (largest column sum of absolute values)
+cudaError_t batch_norm1(int m, int n, const double* X, int64_t ldx, int64_t sx, int batch, double* out,
+                        cudaStream_t st);
+// X_b <- s[b] X_b
+cudaError_t batch_scale(int m, int n, double* X, int64_t ldx, int64_t sx, int batch, const double* s,
+                        cudaStream_t st);
+// X_b <- cx[b] X_b + cz[b] Z_b (cz[b] = 0 leaves X_b as it is), err2[b] = ||X_b,new - X_b||_F^2
+cudaError_t batch_combine(int m, int n, double* X, int64_t ldx, int64_t sx, const double* Z, int64_t ldz, int64_t sz,
+                          int batch, const double* cx, const double* cz, double* partial, int partial_cap,
+                          double* err2, cudaStream_t st);
+cudaError_t batch_add_diag(int n, double* G, int64_t ldg, int64_t sg, int batch, double d, cudaStream_t st);
+cudaError_t batch_symmetrize(int n, double* B, int64_t ldb, int64_t sb, int batch, cudaStream_t st);
+cudaError_t batch_transpose(int m, int n, const double* A, int64_t lda, int64_t sa, double* B, int64_t ldb,
+                            int64_t sb, int batch, cudaStream_t st);
 
 }  // namespace zolo

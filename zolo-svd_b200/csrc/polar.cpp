@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <vector>
 
 #include "coeff.h"
@@ -145,13 +146,15 @@ void newton_schulz_finish(Context& c, int m, int n, double* X, int64_t ldx, Mat 
 }
 
 // Z(b) = X W_b^{-1} (left = false) or W_b^{-1} X (left = true, square X), W_b = L_b L_b^T.
+// strideX: X of batch entry b at X + b*strideX (0: one X shared by the r terms); the left
+// solve takes a shared X only.
 void spd_solve(Context& c, int m, int n, const double* X, int64_t ldx, Mat Lw, DiagInv D, Mat Z, int batch,
-               bool left) {
+               bool left, int64_t strideX = 0) {
   const int64_t ldm = even(m);
   Mat Xc{c.buf("Xc", static_cast<size_t>(ldm) * n * batch), ldm, ldm * n};
   Mat Y{c.buf("Y", static_cast<size_t>(ldm) * n * batch), ldm, ldm * n};
   if (!left) {
-    ck(scale_copy(m, n, 1.0, X, ldx, 0, Xc.p, Xc.ld, Xc.stride, batch, 0.0, c.stream()));
+    ck(scale_copy(m, n, 1.0, X, ldx, strideX, Xc.p, Xc.ld, Xc.stride, batch, 0.0, c.stream()));
     c.stats.launches++;
     trsm_rlt(c, m, n, Lw, Xc, Y, batch, D);
     trsm_rln(c, m, n, Lw, Y, Z, batch, D);
@@ -483,6 +486,271 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     c.stats.ms_h = th.stop();
   }
   c.stats.ms_total = total.stop();
+  return 0;
+}
+
+namespace {
+
+// padded sizes of the batch buckets: multiples of 32 about 1.2x apart
+int bucket_size(int n) {
+  static const int ladder[] = {32,  64,  96,  128, 160, 192,  224,  256,  320,  384,  448,  512,
+                               640, 768, 896, 1024, 1280, 1536, 1792, 2048, 2560, 3072, 3584, 4096};
+  for (int v : ladder)
+    if (n <= v) return v;
+  return (n + 511) / 512 * 512;
+}
+
+constexpr int kMaxBatch = 1024;  // members per launch (the device INFO array holds 1024)
+
+void h2d_bytes(Context& c, void* d, const void* h, size_t bytes) {
+  ck(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c.stream()));
+}
+
+std::vector<double> d2h_vec(Context& c, const double* d, int count) {
+  std::vector<double> h(count);
+  ck(cudaMemcpyAsync(h.data(), d, sizeof(double) * count, cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  return h;
+}
+
+// One bucket: B members padded to MB x NB, solved together (pqdwhfacs.f90:318-457 per member).
+void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const int* m, const int* n,
+                 const double* const* dA, const int64_t* lda, double* const* dQ, const int64_t* ldq,
+                 double* const* dH, const int64_t* ldh, int* info, int* iterations, BatchStats* bs) {
+  const int B = static_cast<int>(idx.size());
+  const cudaStream_t st = c.stream();
+  const int64_t ldp = MB, sP = ldp * NB, ldn = NB, sN = ldn * NB;
+  double* Ap = c.buf("bat_a", static_cast<size_t>(sP) * B);
+  double* X = c.buf("bat_x", static_cast<size_t>(sP) * B);
+  double* vals = c.buf("bat_vec", static_cast<size_t>(8) * B);
+  double* part = c.buf("bat_part", 8192);
+  const size_t mem_doubles = (sizeof(BatchMember) * B + 7) / 8;
+  auto* dmem = reinterpret_cast<BatchMember*>(c.buf("bat_mem", mem_doubles));
+  std::vector<BatchMember> hm(B);
+  for (int b = 0; b < B; ++b) {
+    const int i = idx[b];
+    hm[b] = BatchMember{m[i], n[i], dA[i], lda[i], 0.0, dQ[i], ldq[i], dH ? dH[i] : nullptr, dH ? ldh[i] : 0};
+  }
+  // pad with tau = ||A||_F / sqrt(n), a value inside [sigma_min, sigma_max]
+  h2d_bytes(c, dmem, hm.data(), sizeof(BatchMember) * B);
+  ck(batch_pack(dmem, B, MB, NB, Ap, ldp, sP, st));
+  ck(batch_frob2(MB, NB, Ap, ldp, sP, B, part, 8192, vals, st));
+  const std::vector<double> fa = d2h_vec(c, vals, B);
+  bool padded = false;
+  for (int b = 0; b < B; ++b) {
+    hm[b].tau = std::sqrt(fa[b] / hm[b].n);
+    padded = padded || hm[b].n < NB;
+  }
+  if (padded) {
+    h2d_bytes(c, dmem, hm.data(), sizeof(BatchMember) * B);
+    ck(batch_pack(dmem, B, MB, NB, Ap, ldp, sP, st));
+  }
+  c.stats.launches += padded ? 4 : 3;
+
+  // ---- bounds, PQDWHFACS form: alpha = ||A'||_F, beta = ||X0||_1 / (sqrt(NB) ||R^-1||_1) ----
+  ck(batch_frob2(MB, NB, Ap, ldp, sP, B, part, 8192, vals, st));
+  std::vector<double> alpha = d2h_vec(c, vals, B);
+  std::vector<double> hv(8 * B, 0.0);
+  std::vector<char> done(B, 0);
+  for (int b = 0; b < B; ++b) {
+    alpha[b] = std::sqrt(alpha[b]);
+    if (!(alpha[b] > 0.0) || !std::isfinite(alpha[b])) {
+      info[idx[b]] = 1;
+      done[b] = 1;
+    }
+    hv[b] = done[b] ? 1.0 : 1.0 / alpha[b];
+  }
+  h2d(c, vals, hv.data(), B);
+  ck(scale_copy(MB, NB, 1.0, Ap, ldp, sP, X, ldp, sP, B, 0.0, st));
+  ck(batch_scale(MB, NB, X, ldp, sP, B, vals, st));
+  ck(batch_norm1(MB, NB, X, ldp, sP, B, vals + B, st));
+  double* Xq = c.buf("bat_xq", static_cast<size_t>(sP) * B);
+  ck(scale_copy(MB, NB, 1.0, X, ldp, sP, Xq, ldp, sP, B, 0.0, st));
+  c.stats.launches += 5;
+  double* tau = c.buf("bat_tau", static_cast<size_t>(NB) * B);
+  const int np = (NB + 31) / 32;
+  double* T = c.buf("bat_t", static_cast<size_t>(np) * 1024 * B);
+  geqrf(c, MB, NB, -1, Mat{Xq, ldp, sP}, tau, T, B);
+  double* Lt = c.buf("bat_lt", static_cast<size_t>(sN) * B);
+  double* Id = c.buf("bat_i", static_cast<size_t>(sN) * B);
+  double* Ri = c.buf("bat_ri", static_cast<size_t>(sN) * B);
+  ck(batch_transpose(NB, NB, Xq, ldp, sP, Lt, ldn, sN, B, st));
+  ck(set_identity(NB, NB, Id, ldn, sN, B, 1.0, st));
+  c.stats.launches += 2;
+  const int64_t sD = static_cast<int64_t>(nblocks(NB)) * 4096;
+  DiagInv D{c.buf("bat_dinv", static_cast<size_t>(sD) * B), sD};
+  diag_inverses(c, NB, Mat{Lt, ldn, sN}, B, D);
+  trsm_rlt(c, NB, NB, Mat{Lt, ldn, sN}, Mat{Id, ldn, sN}, Mat{Ri, ldn, sN}, B, D);
+  ck(batch_norm1(NB, NB, Ri, ldn, sN, B, vals + 2 * B, st));
+  c.stats.launches++;
+  const std::vector<double> nv = d2h_vec(c, vals + B, 2 * B);
+  std::vector<double> lowk(B, 1.0), err(B, 1.0);
+  std::vector<int> its(B, 0);
+  for (int b = 0; b < B; ++b) {
+    const double beta = nv[b] / (std::sqrt(static_cast<double>(NB)) * nv[B + b]);
+    if (!done[b] && (!std::isfinite(beta) || !(beta > 0.0))) {
+      info[idx[b]] = 1;
+      done[b] = 1;
+    }
+    lowk[b] = done[b] ? 1.0 : beta;
+  }
+  double flops = 4.0 / 3.0 * NB * static_cast<double>(NB) * NB + 2.0 * MB * static_cast<double>(NB) * NB;
+  double useful = 0.0;
+  for (int b = 0; b < B; ++b) {
+    const double mm = m[idx[b]], nn = n[idx[b]];
+    useful += 4.0 / 3.0 * nn * nn * nn + 2.0 * mm * nn * nn;
+  }
+  flops *= B;
+
+  // ---- the iteration, all members together ----
+  const double eps = eps_precision();
+  const double tol1 = 10.0 * eps / 2.0;
+  const double tol2 = std::exp(std::log(tol1) / 3.0);
+  const int maxit = 12;
+  const int mp = MB;  // the sqrt(c) I block of the QR stack starts at row MB (even)
+  const int64_t ldw = even(static_cast<int64_t>(mp) + NB), sW = ldw * NB;
+  Mat W{c.buf("bat_w", static_cast<size_t>(sW) * B), ldw, sW};
+  Mat Qf{c.buf("bat_qf", static_cast<size_t>(sW) * B), ldw, sW};
+  Mat Z{c.buf("bat_z", static_cast<size_t>(sP) * B), ldp, sP};
+  Mat G{c.buf("bat_g", static_cast<size_t>(sN) * B), ldn, sN};
+  DiagInv Dg{c.buf("bat_dinv2", static_cast<size_t>(sD) * B), sD};
+  int* dinfo = c.dinfo();
+  std::vector<double> ak(B), bk(B), ckv(B), ln(B);
+  std::vector<double> cx(B), cz(B);
+  int it = 0;
+  while (true) {
+    bool any = false, use_qr = false;
+    for (int b = 0; b < B; ++b) {
+      if (done[b]) continue;
+      any = true;
+      qdwh_weights(lowk[b], &ak[b], &bk[b], &ckv[b], &ln[b]);
+      use_qr = use_qr || ckv[b] > 100.0;
+    }
+    if (!any) break;
+    if (!use_qr) {
+      for (int b = 0; b < B; ++b) hv[b] = done[b] ? 0.0 : ckv[b];
+      h2d(c, vals, hv.data(), B);
+      gemm(c, 1, 0, NB, NB, MB, 1.0, Mat{X, ldp, sP}, Mat{X, ldp, sP}, 0.0, G, B, vals, 1, 0);
+      ck(batch_add_diag(NB, G.p, G.ld, G.stride, B, 1.0, st));
+      ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * B, st));
+      c.stats.launches += 2;
+      potrf(c, NB, G, B, dinfo, Dg);
+      std::vector<int> pin(B, 0);
+      ck(cudaMemcpyAsync(pin.data(), dinfo, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
+      ck(cudaStreamSynchronize(st));
+      bool fail = false;
+      for (int b = 0; b < B; ++b) fail = fail || (!done[b] && pin[b] != 0);
+      if (fail) {
+        use_qr = true;  // not numerically SPD for some member: this step takes the QR form
+      } else {
+        spd_solve(c, MB, NB, X, ldp, G, Dg, Z, B, false, sP);
+        for (int b = 0; b < B; ++b) {
+          cx[b] = done[b] ? 1.0 : bk[b] / ckv[b];
+          cz[b] = done[b] ? 0.0 : ak[b] - bk[b] / ckv[b];
+        }
+        flops += B * (2.0 * MB * static_cast<double>(NB) * NB + NB * static_cast<double>(NB) * NB / 3.0 +
+                      static_cast<double>(MB) * NB * NB);
+        for (int b = 0; b < B; ++b) {
+          if (done[b]) continue;
+          const double mm = m[idx[b]], nn = n[idx[b]];
+          useful += 3.0 * mm * nn * nn + nn * nn * nn / 3.0;
+        }
+      }
+    }
+    if (use_qr) {
+      for (int b = 0; b < B; ++b) hv[b] = done[b] ? 1.0 : 1.0 / std::sqrt(ckv[b]);
+      h2d(c, vals, hv.data(), B);
+      ck(form_stack(MB, mp, NB, X, ldp, W.p, W.ld, W.stride, vals, 0.0, B, st, 0, sP));
+      c.stats.launches++;
+      geqrf(c, mp + NB, NB, mp, W, tau, T, B);
+      orgqr(c, mp + NB, NB, mp, W, T, Qf, B);
+      q1q2t(c, MB, mp, NB, Qf, Z, B);
+      for (int b = 0; b < B; ++b) {
+        const double sck = done[b] ? 1.0 : std::sqrt(ckv[b]);
+        cx[b] = done[b] ? 1.0 : bk[b] / ckv[b];
+        cz[b] = done[b] ? 0.0 : (ak[b] - bk[b] / ckv[b]) / sck;
+      }
+      flops += B * (4.0 * MB * static_cast<double>(NB) * NB + static_cast<double>(NB) * NB * NB);
+      for (int b = 0; b < B; ++b) {
+        if (done[b]) continue;
+        const double mm = m[idx[b]], nn = n[idx[b]];
+        useful += 4.0 * mm * nn * nn + nn * nn * nn;
+      }
+    }
+    for (int b = 0; b < B; ++b) {
+      hv[B + b] = cx[b];
+      hv[2 * B + b] = cz[b];
+    }
+    h2d(c, vals + B, hv.data() + B, 2 * B);
+    ck(batch_combine(MB, NB, X, ldp, sP, Z.p, Z.ld, Z.stride, B, vals + B, vals + 2 * B, part, 8192, vals + 3 * B,
+                     st));
+    c.stats.launches += 2;
+    const std::vector<double> e2 = d2h_vec(c, vals + 3 * B, B);
+    ++it;
+    for (int b = 0; b < B; ++b) {
+      if (done[b]) continue;
+      err[b] = std::sqrt(e2[b]);
+      lowk[b] = ln[b];
+      ++its[b];
+      // pqdwhfacs.f90:359: continue while ERR > TOL1^(1/3) or |1 - L| > TOL1, IT <= 12
+      const bool more = (err[b] > tol2 || std::fabs(1.0 - lowk[b]) > tol1) && its[b] <= maxit;
+      if (!more) done[b] = 1;
+    }
+  }
+  // ---- H' = sym(Q'^T A') and the unpadded outputs ----
+  double* Hp = nullptr;
+  if (dH) {
+    Hp = c.buf("bat_h", static_cast<size_t>(sN) * B);
+    gemm(c, 1, 0, NB, NB, MB, 1.0, Mat{X, ldp, sP}, Mat{Ap, ldp, sP}, 0.0, Mat{Hp, ldn, sN}, B);
+    ck(batch_symmetrize(NB, Hp, ldn, sN, B, st));
+    c.stats.launches++;
+    flops += B * 2.0 * MB * static_cast<double>(NB) * NB;
+    for (int b = 0; b < B; ++b) useful += 2.0 * m[idx[b]] * static_cast<double>(n[idx[b]]) * n[idx[b]];
+  }
+  ck(batch_unpack(dmem, B, MB, NB, X, ldp, sP, Hp, ldn, sN, st));
+  c.stats.launches++;
+  for (int b = 0; b < B; ++b)
+    if (iterations) iterations[idx[b]] = its[b];
+  bs->buckets++;
+  bs->max_iterations = std::max(bs->max_iterations, it);
+  bs->flops += flops;
+  bs->flops_useful += useful;
+}
+
+}  // namespace
+
+int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* const* dA, const int64_t* lda,
+               double* const* dQ, const int64_t* ldq, double* const* dH, const int64_t* ldh, int* info,
+               int* iterations, BatchStats* bs) {
+  if (count < 0) return -2;
+  for (int i = 0; i < count; ++i) {
+    if (n[i] < 1 || m[i] < n[i]) return -3;
+    if (lda[i] < m[i] || ldq[i] < m[i] || (dH && ldh[i] < n[i])) return -4;
+    info[i] = 0;
+  }
+  BatchStats local;
+  if (!bs) bs = &local;
+  *bs = BatchStats{};
+  c.stats = Stats{};
+  EventTimer total(c.stream());
+  std::map<int, std::vector<int>> buckets;
+  for (int i = 0; i < count; ++i) buckets[bucket_size(n[i])].push_back(i);
+  for (const auto& kv : buckets) {
+    const int NB = kv.first;
+    const std::vector<int>& all = kv.second;
+    for (size_t off = 0; off < all.size(); off += kMaxBatch) {
+      const std::vector<int> idx(all.begin() + off, all.begin() + std::min(all.size(), off + kMaxBatch));
+      int MB = NB;
+      for (int i : idx) MB = std::max(MB, m[i] + NB - n[i]);
+      MB = (MB + 31) / 32 * 32;
+      qdwh_bucket(c, idx, MB, NB, m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, bs);
+    }
+  }
+  bs->ms = total.stop();
+  c.stats.ms_total = bs->ms;
+  c.stats.flops = bs->flops_useful;
+  c.stats.flops_exec_delta = bs->flops - bs->flops_useful;
+  c.stats.iterations = bs->max_iterations;
   return 0;
 }
 

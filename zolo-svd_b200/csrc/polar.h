@@ -32,6 +32,24 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
 int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double beta, const double* dA, int64_t lda,
             double* dQ, int64_t ldq, double* dH, int64_t ldh, int maxit = 6);
 
+// QDWH-PD (PQDWHFACS steps and bounds, SYM = 'N', SIGMA = 0) of `count` matrices of
+// different sizes.  Members are grouped into buckets of one padded size NB (a ladder of
+// multiples of 32) and padded exactly: A' = [[A, 0], [0, tau I], [0, 0]] with
+// tau = ||A||_F / sqrt(n), which lies in [sigma_min, sigma_max], so the condition number
+// is unchanged and polar(A') = diag(polar(A), I), H' = diag(H, tau I).  Each bucket runs
+// as one batched solve with per-member weights and convergence.  info[i] = 0, or > 0
+// when member i's bounds or Cholesky failed (its outputs are then undefined).
+struct BatchStats {
+  int buckets = 0;
+  int max_iterations = 0;
+  double flops = 0.0;       // executed FP64 flops, padding included
+  double flops_useful = 0.0;  // the same work counted on the unpadded sizes
+  double ms = 0.0;
+};
+int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* const* dA, const int64_t* lda,
+               double* const* dQ, const int64_t* ldq, double* const* dH, const int64_t* ldh, int* info,
+               int* iterations, BatchStats* bs);
+
 // H = (Q^T A + A^T Q)/2
 void form_h(Context& c, int m, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, double* dH,
             int64_t ldh);
