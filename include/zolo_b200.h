@@ -95,11 +95,12 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
 /* ZOLO_OPT_NS_FINISH: 0 (default) = the reference's stopping rule
  * (pzolopd1.f90:381-397: iterate until ||X_{k+1} - X_k||_F <= (5 eps)^(1/(2r+1))).
  * 1 = before each Cholesky-form Zolo-PD iteration, measure e = ||X^T X - I||_F/sqrt(n)
- * from the Gram matrix that iteration forms anyway; once e <= 5e-3, finish with
+ * from the Gram matrix that iteration forms anyway; once e <= 0.1, finish with
  * FP64 Newton-Schulz steps X <- X (3I - X^T X)/2 instead of further Zolo
- * iterations (1 to 3 steps, as many as e -> 1.5 e^2 needs to reach 1e-16).  The
- * polar factor of X is that of A, so the result agrees with the reference rule's
- * to rounding.  No reference counterpart. */
+ * iterations, re-measuring e before each step and stopping at rounding level
+ * (max(1e-14, eps sqrt(m)/2), or when a step no longer halves e; at most 12 steps,
+ * none when e is already there).  The polar factor of X is that of A, so the result
+ * agrees with the reference rule's to rounding.  No reference counterpart. */
 #define ZOLO_OPT_NS_FINISH 2
 int zolo_set_option(zolo_handle_t handle, int option, int value);
 

@@ -63,6 +63,11 @@ struct EventTimer {
 
 int npanels(int n) { return (n + 31) / 32; }
 
+// Newton-Schulz finish of Zolo-PD (ZOLO_OPT_NS_FINISH): entry threshold on
+// ||X^T X - I||_F / sqrt(n) and the cap on the number of steps
+constexpr double kNsEnter = 0.1;
+constexpr int kNsMaxSteps = 12;
+
 // Q1 * Q2^T of the explicit Q of the stacked matrix (Q2 starts at row mp, upper triangular).
 void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
   gemm(c, 0, 1, m, n, n, 1.0, Qf, Qf.at(mp, 0), 0.0, Z, batch, nullptr, 0, 1);
@@ -112,23 +117,19 @@ void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx
   c.stats.flops_exec_delta += executed - rk * (4.0 * dm * dn * dn + dn * dn * dn);
 }
 
-// Finish of the polar iteration by FP64 Newton-Schulz steps X <- X (3I - X^T X)/2
-// (quadratic: e -> 1.5 e^2 for e = ||X^T X - I||_F / sqrt(n)).  On entry G holds
-// the lower triangle of X^T X and e0 its measured e; the number of steps is the
-// smallest that takes the predicted e below 1e-16 (at most 3 for e0 <= 5e-3).
-// Records the steps as branch 3 after the `it` Zolo iterations.
+// Finish of the polar iteration by FP64 Newton-Schulz steps X <- X (3I - X^T X)/2.
+// e = ||X^T X - I||_F / sqrt(n) is measured before every step (the Gram is the step's
+// own first half) and the steps stop once e reaches the rounding floor
+// max(1e-14, eps sqrt(m) / 2), once a step no longer halves e (rounding level), or
+// after kNsMaxSteps.  Near convergence e -> 0.75 e^2; from e = 0.1 that is four steps.  On entry G holds the lower triangle of X^T X and e0 its
+// e.  Records the steps as branch 3 after the `it` Zolo iterations.
 void newton_schulz_finish(Context& c, int m, int n, double* X, int64_t ldx, Mat G, Mat Z, double e0, int it) {
-  int steps = 1;
-  for (double e = 1.5 * e0 * e0; e > 1e-16 && steps < 3; e = 1.5 * e * e) ++steps;
+  const double floor_e = std::max(1e-14, 0.5 * eps_precision() * std::sqrt(static_cast<double>(m)));
   double* scal = c.dscal();
-  double ek = e0;
-  for (int k = 0; k < steps; ++k) {
-    if (k > 0) {
-      gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
-      c.stats.flops += static_cast<double>(m) * n * n;
-    }
+  double e = e0, e_prev = 2.0 * e0 + 1.0;
+  for (int k = 0; k < kNsMaxSteps && e > floor_e && e < 0.5 * e_prev; ++k) {
+    e_prev = e;
     ck(ns_prepare(n, G.p, G.ld, c.dpartial(), scal + 2, 1, c.stream()));
-    if (k > 0) ek = std::sqrt(d2h(c, scal + 2) / n);
     gemm(c, 0, 0, m, n, n, 1.0, Mat{X, ldx, 0}, G, 0.0, Mat{Z.p, Z.ld, 0}, 1);
     ck(scale_copy(m, n, 1.0, Z.p, Z.ld, 0, X, ldx, 0, 1, 0.0, c.stream()));
     c.stats.launches += 3;
@@ -137,11 +138,17 @@ void newton_schulz_finish(Context& c, int m, int n, double* X, int64_t ldx, Mat 
     if (slot < 16) {
       c.stats.branch[slot] = 3;
       c.stats.con[slot] = 1.0;
-      c.stats.err[slot] = ek;
+      c.stats.err[slot] = e;
     }
     c.stats.ns_steps++;
+    // the next Gram: the measurement that decides whether another step is needed
+    gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+    ck(ns_prepare(n, G.p, G.ld, c.dpartial(), scal + 2, 0, c.stream()));
+    c.stats.launches += 2;
+    c.stats.flops += static_cast<double>(m) * n * n;
+    e = std::sqrt(d2h(c, scal + 2) / n);
   }
-  // the SYRK of the first step was counted by the Cholesky branch that measured e0
+  // the Gram that measured e0 was counted by the Cholesky branch's SYRK
   c.stats.flops += static_cast<double>(m) * n * n;
 }
 
@@ -401,12 +408,12 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     if (!use_qr) {
       gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       if (ns_finish) {
-        // G = X^T X is in hand: when X is already within 5e-3 of orthogonal, the rest of
-        // the iteration is FP64 Newton-Schulz (the polar factor of X is that of A)
+        // G = X^T X is in hand: once X is within 0.1 of orthogonal (RMS of sigma^2 - 1),
+        // the rest of the iteration is FP64 Newton-Schulz (the polar factor of X is that of A)
         ck(ns_prepare(n, G.p, G.ld, part, scal + 2, 0, c.stream()));
         c.stats.launches += 2;
         const double e0 = std::sqrt(d2h(c, scal + 2) / n);
-        if (e0 <= 5e-3) {
+        if (e0 <= kNsEnter) {
           newton_schulz_finish(c, m, n, X, ldx, G, Z, e0, it);
           c.stats.ns_finish = 1;
           break;
