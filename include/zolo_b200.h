@@ -185,6 +185,15 @@ int zolo_qdwh_dev(zolo_handle_t h, char sym, int m, int n, double sigma, const d
 int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, const double* const* dA,
                         const int64_t* lda, double* const* dQ, const int64_t* ldq, double* const* dH,
                         const int64_t* ldh, int* info, int* iterations);
+/* The reference driver's sequence in one call (test_zolodrv1.f90:167-198: the bounds,
+ * then PZOLOPD1 with SYM = 'N'), plus H when dH is not NULL: alpha = ||A||_F and
+ * beta = 1/(sqrt(n) ||R^{-1}||_1) as zolo_bounds_dev mode 1, then Zolo-PD with rk
+ * terms.  The Householder QR of A/alpha that gives beta is reused by the first Zolo-PD
+ * iteration when it takes the QR form with ZOLO_OPT_SHARED_QR (X0 = A/(alpha beta) has
+ * the same Q), which saves one QR of A.  alpha, beta and the iteration record are in
+ * zolo_get_stats.  Returns INFO. */
+int zolo_polar_dev(zolo_handle_t h, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq,
+                   double* dH, int64_t ldh);
 /* Zolo-PD (PZOLOPD1 semantics) on device arrays; dH may be NULL.  Returns INFO. */
 int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
                       int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh);

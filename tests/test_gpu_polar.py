@@ -191,6 +191,32 @@ def test_solves_are_bitwise_reproducible():
     assert torch.equal(outs[0][3], outs[1][3])
 
 
+@pytest.mark.parametrize("m,n,kappa", [(300, 300, 1e12), (420, 250, 1e10), (129, 129, 1e16)])
+def test_polar_dev_matches_bounds_then_pzolopd1(m, n, kappa):
+    """zolo_polar_dev (bounds + Zolo-PD + H sharing the QR of A/alpha) against the two
+    separate calls: same alpha, beta and branch sequence, the same iterate to rounding."""
+    import torch
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a, _, _ = zo.make_matrix(n, s, 600 + m + n, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    dq0, dq1 = torch.zeros_like(da), torch.zeros_like(da)
+    dh0 = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    dh1 = torch.zeros_like(dh0)
+    torch.cuda.synchronize()
+    al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)
+    zb.pzolopd1_dev(h, "N", 8, m, n, al, be, da.data_ptr(), m, dq0.data_ptr(), m, dh0.data_ptr(), n)
+    st0 = h.stats()
+    assert zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq1.data_ptr(), m, dh1.data_ptr(), n) == 0
+    st1 = h.stats()
+    h.close()
+    assert st1["alpha"] == al and st1["beta"] == be
+    assert st1["branches"] == st0["branches"] and st1["branches"][0] == "QR"
+    q0, q1 = zb.device_to_colmajor(dq0), zb.device_to_colmajor(dq1)
+    check_pd(a, q1, zb.device_to_colmajor(dh1), n)
+    assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
+
+
 def test_set_option_rejects_unknown():
     h = zb.Handle(0)
     with pytest.raises(zb.ZoloError):

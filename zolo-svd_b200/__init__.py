@@ -96,6 +96,8 @@ _SIGS = [
     ("zolo_qdwh_batch_dev", C.c_int, [C.c_void_p, C.c_int, c_int_p, c_int_p, C.POINTER(C.c_void_p),
                                       C.POINTER(C.c_int64), C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_void_p), C.POINTER(C.c_int64), c_int_p, c_int_p]),
+    ("zolo_polar_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                                 C.c_int64, C.c_void_p, C.c_int64]),
     ("zolo_qdwh_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64,
                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int]),
     ("zolo_pzolopd1_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -369,6 +371,12 @@ def qdwh_batch_dev(h: Handle, members, with_h: bool = True):
     its = (C.c_int * k)()
     _ck("zolo_qdwh_batch_dev", lib().zolo_qdwh_batch_dev(h.ptr, k, m, n, a, lda, q, ldq, hh, ldh, info, its))
     return list(info), list(its)
+
+
+def polar_dev(h: Handle, rk: int, m: int, n: int, dA: int, lda: int, dQ: int, ldq: int, dH: int = 0,
+              ldh: int = 1) -> int:
+    """Bounds + Zolo-PD (+ H) in one call, sharing the QR of A/alpha; returns INFO."""
+    return _ck("zolo_polar_dev", lib().zolo_polar_dev(h.ptr, rk, m, n, dA, lda, dQ, ldq, dH or None, ldh))
 
 
 def pzolopd1_dev(h: Handle, sym: str, rk: int, m: int, n: int, alpha: float, beta: float, dA: int, lda: int,

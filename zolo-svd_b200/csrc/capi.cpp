@@ -371,6 +371,13 @@ int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, 
   });
 }
 
+int zolo_polar_dev(zolo_handle_t h, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq,
+                   double* dH, int64_t ldh) {
+  if (m < n) return -3;
+  if (lda < std::max(1, m) || ldq < std::max(1, m) || (dH && ldh < std::max(1, n))) return -6;
+  return guarded(h, [&](Context& c) { return zolo::zolo_polar(c, rk, m, n, dA, lda, dQ, ldq, dH, ldh); });
+}
+
 int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
                       int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh) {
   return guarded(h, [&](Context& c) {

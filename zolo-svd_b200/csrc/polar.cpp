@@ -86,15 +86,24 @@ void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
 // Flops: QR of X 4mn^2 - 4n^3/3, per term 4n^3/3 (structured QR and Q) + n^3
 // (triangular product), and 2mn^2 for the final product -- against
 // r (4mn^2 + n^3) for r independent (m+n) x n stacks.
+// With `pf`, X = (the matrix pf factors) / scale: Q_x is pf's Q and R_x = R / scale, and
+// d_sqrtc must already hold scale * sqrt(c_j) ([R/scale; sqrt(c) I] and [R; scale sqrt(c) I]
+// have the same Q factor).
 void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx, Mat W, Mat Qf, Mat Z, double* tau,
-                          double* T, const double* d_sqrtc, const double* hw, double fone, int rk) {
+                          double* T, const double* d_sqrtc, const double* hw, double fone, int rk,
+                          const Prefactored* pf = nullptr) {
   const int64_t ldn = even(n);
   Mat Xq{c.buf("zq_x", static_cast<size_t>(ldx) * n), ldx, 0};
   Mat Qx{c.buf("zq_q", static_cast<size_t>(ldx) * n), ldx, 0};
-  ck(scale_copy(m, n, 1.0, X, ldx, 0, Xq.p, Xq.ld, 0, 1, 0.0, c.stream()));
-  c.stats.launches++;
-  geqrf(c, m, n, -1, Xq, tau, T, 1);
-  orgqr(c, m, n, -1, Xq, T, Qx, 1);
+  if (pf) {
+    Xq = Mat{const_cast<double*>(pf->W), pf->ldw, 0};
+    orgqr(c, m, n, -1, Xq, pf->T, Qx, 1);
+  } else {
+    ck(scale_copy(m, n, 1.0, X, ldx, 0, Xq.p, Xq.ld, 0, 1, 0.0, c.stream()));
+    c.stats.launches++;
+    geqrf(c, m, n, -1, Xq, tau, T, 1);
+    orgqr(c, m, n, -1, Xq, T, Qx, 1);
+  }
   // W and Qf hold r stacks of (m + n) x n with m >= n: room for r stacks [R_x; 0; sqrt(c_j) I]
   // of ldn + n rows (the identity block at the even row offset ldn)
   const int mt = static_cast<int>(ldn), mtot = mt + n;
@@ -112,8 +121,8 @@ void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx
   }
   gemm(c, 0, 0, m, n, n, 1.0, Qx, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
   const double dm = m, dn = n;
-  const double executed =
-      4.0 * dm * dn * dn - 4.0 * dn * dn * dn / 3.0 + rk * (7.0 * dn * dn * dn / 3.0) + 2.0 * dm * dn * dn;
+  const double executed = (pf ? 2.0 : 4.0) * dm * dn * dn - (pf ? 2.0 : 4.0) * dn * dn * dn / 3.0 +
+                          rk * (7.0 * dn * dn * dn / 3.0) + 2.0 * dm * dn * dn;
   c.stats.flops_exec_delta += executed - rk * (4.0 * dm * dn * dn + dn * dn * dn);
 }
 
@@ -359,7 +368,7 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
 }
 
 int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double beta, const double* dA, int64_t lda,
-            double* dQ, int64_t ldq, double* dH, int64_t ldh, int maxit) {
+            double* dQ, int64_t ldq, double* dH, int64_t ldh, int maxit, const Prefactored* pf) {
   if (m < n) return -3;
   if (rk < 1 || rk > 8) return -2;
   if (m == 0 || n == 0) return 0;
@@ -442,12 +451,14 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     const double con_next = zolo_next_con(con, coeff.data(), rk, fone);
     bool shared = false;
     if (use_qr) {
-      for (int b = 0; b < rk; ++b) hv[b] = std::sqrt(coeff[2 * b]);
+      shared = c.zolo_shared_qr != 0;
+      // the first iteration may reuse the QR of A/alpha: X0 = (A/alpha)/beta
+      const Prefactored* pfi = (shared && it == 0) ? pf : nullptr;
+      for (int b = 0; b < rk; ++b) hv[b] = std::sqrt(coeff[2 * b]) * (pfi ? beta : 1.0);
       h2d(c, dvec, hv.data(), rk);
       for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b] / std::sqrt(coeff[2 * b]);
-      shared = c.zolo_shared_qr != 0;
       if (shared) {
-        zolo_terms_shared_qr(c, m, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk);
+        zolo_terms_shared_qr(c, m, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk, pfi);
       } else {
         ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk, c.stream()));
         c.stats.launches++;
@@ -494,6 +505,32 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   }
   c.stats.ms_total = total.stop();
   return 0;
+}
+
+int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq, double* dH,
+               int64_t ldh) {
+  if (m < n) return -3;
+  if (rk < 1 || rk > 8) return -2;
+  if (m == 0 || n == 0) return 0;
+  EventTimer total(c.stream());
+  double alpha = 0.0, beta = 0.0;
+  EventTimer tb(c.stream());
+  const int binfo = bounds(c, m, n, 0.0, dA, lda, BOUNDS_ZOLOPD, &alpha, &beta);
+  const double ms_bounds = tb.stop();
+  const double bflops = 4.0 / 3.0 * static_cast<double>(n) * n * n + 2.0 * m * static_cast<double>(n) * n;
+  if (binfo != 0) {
+    c.stats = Stats{};
+    c.stats.info = binfo;
+    return binfo;
+  }
+  // bounds left the factored A/alpha in its workspace ("bnd_x", ld even(m)) and the panel factors in "bnd_t"
+  const Prefactored pf{c.buf("bnd_x", static_cast<size_t>(even(m)) * n), even(m),
+                       c.buf("bnd_t", static_cast<size_t>(npanels(n)) * 1024)};
+  const int info = zolo_pd(c, 'N', rk, m, n, alpha, beta, dA, lda, dQ, ldq, dH, ldh, 6, &pf);
+  c.stats.ms_bounds = ms_bounds;
+  c.stats.flops += bflops;
+  c.stats.ms_total = total.stop();
+  return info;
 }
 
 namespace {

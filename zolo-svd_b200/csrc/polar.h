@@ -28,9 +28,25 @@ struct QdwhOpts {
 int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh,
          const QdwhOpts& o);
 
-// Zolo-PD of As/(alpha*beta) with rk terms (pzolopd1.f90:280-487); H as above.
+// A Householder QR of A/alpha already computed (by bounds): the factored matrix W
+// (R on and above the diagonal, reflectors below; ld ldw) and its panel factors T.
+struct Prefactored {
+  const double* W;
+  int64_t ldw;
+  const double* T;
+};
+
+// Zolo-PD of As/(alpha*beta) with rk terms (pzolopd1.f90:280-487); H as above.  With
+// `pf` (the QR of A/alpha) the first iteration, if it takes the QR form with the QR of
+// X shared by the terms, reuses it: X0 = A/(alpha beta) has the same Q and R/beta.
 int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double beta, const double* dA, int64_t lda,
-            double* dQ, int64_t ldq, double* dH, int64_t ldh, int maxit = 6);
+            double* dQ, int64_t ldq, double* dH, int64_t ldh, int maxit = 6, const Prefactored* pf = nullptr);
+
+// bounds (ZOLOPD form) + Zolo-PD + H in one call, the flow of the reference's driver
+// (test_zolodrv1.f90:167-198): the QR of A/alpha that gives beta is reused by the first
+// Zolo-PD iteration.  Returns INFO; alpha and beta are reported in the stats.
+int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq, double* dH,
+               int64_t ldh);
 
 // QDWH-PD (PQDWHFACS steps and bounds, SYM = 'N', SIGMA = 0) of `count` matrices of
 // different sizes.  Members are grouped into buckets of one padded size NB (a ladder of
