@@ -102,6 +102,14 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * none when e is already there).  The polar factor of X is that of A, so the result
  * agrees with the reference rule's to rounding.  No reference counterpart. */
 #define ZOLO_OPT_NS_FINISH 2
+/* ZOLO_OPT_CHOL_INVERSE: 0 (default) = each Cholesky-form term solves
+ * X (X^T X + c_j I)^{-1} with two triangular solves (zolochol.f90:87-113); 1 = the
+ * terms' inverses L_j^{-T} L_j^{-1} (triangular inverse + one lower-triangle product,
+ * 4n^3/3 per term) are summed into S = sum_j w_j (X^T X + c_j I)^{-1} and the iteration
+ * takes one Z = X S, about 6n^3 fewer flops per iteration for r = 8.  These matrices
+ * are well conditioned in the Cholesky iterations (condition <= CON^2, CON <= 1e3), so
+ * both forms agree to rounding.  SYM = 'S' keeps the solves.  No reference counterpart. */
+#define ZOLO_OPT_CHOL_INVERSE 3
 int zolo_set_option(zolo_handle_t handle, int option, int value);
 
 /* ---- host scalar routines (no GPU needed) ---- */
@@ -222,7 +230,8 @@ int zolo_zoloeig_dev(zolo_handle_t h, int n, const double* dQ, int64_t ldq, cons
 
 /* ---- kernel-level entry points (building blocks, used by the parity tests) ---- */
 /* C = alpha op(A) op(B) + beta C (PDGEMM on a 1x1 grid); tri = lower-triangle-only output,
- * kfrom_n = op(B) is lower triangular (TRMM-like skip). */
+ * kfrom_n = 1: op(B) is lower triangular (TRMM-like skip of k < column);
+ * kfrom_n = 2: op(A) is upper triangular (skip of k < row). */
 int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
                    int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
                    int kfrom_n);
@@ -231,6 +240,9 @@ int zolo_dpotrf_dev(zolo_handle_t h, int n, double* dA, int64_t lda);
 /* Y = X L^{-T} (trans = 'T') or Y = X L^{-1} (trans = 'N'); X is overwritten (workspace). */
 int zolo_dtrsm_dev(zolo_handle_t h, char trans, int m, int n, const double* dL, int64_t ldl, double* dX, int64_t ldx,
                    double* dY, int64_t ldy);
+/* Y = L^{-1} for lower-triangular L (PDTRTRI 'L','N' on a 1x1 grid; only L's lower triangle
+ * is read; Y's upper triangle is set to zero). Returns 0, or -i for a bad argument i. */
+int zolo_dtrtri_dev(zolo_handle_t h, int n, const double* dL, int64_t ldl, double* dY, int64_t ldy);
 /* Structured Householder QR (MPDGEQRF, mpdgeqrf.f:5-324): mtot x n in place; m_top < 0 = unstructured.
  * dT receives ceil(n/32) blocks of 32x32 compact-WY factors. */
 int zolo_dgeqrf_dev(zolo_handle_t h, int mtot, int n, int m_top, double* dW, int64_t ldw, double* dtau, double* dT);

@@ -139,6 +139,45 @@ def test_dgemm_triangular_operand_skip(h):
     assert np.allclose(host(dc), ref, rtol=0, atol=4 * n * EPS * (np.abs(q1) @ np.abs(q2.T)).max())
 
 
+def test_dgemm_row_triangular_skip(h):
+    """kfrom_n = 2: op(A) = Y^T with Y lower triangular, so row i of op(A) is zero for
+    k < i; with a lower-triangle output this is Y^T Y of the explicit-inverse Cholesky form."""
+    rng = np.random.default_rng(4)
+    n = 333
+    y = np.tril(rng.standard_normal((n, n)))
+    c0 = rng.standard_normal((n, n))
+    dy, dc = dev(y), dev(c0)
+    r = zb.lib().zolo_dgemm_dev(h.ptr, b"T", b"N", n, n, n, -0.5, dy.data_ptr(), n, dy.data_ptr(), n, 0.0,
+                                dc.data_ptr(), n, 1, 2)
+    assert r == 0
+    got = host(dc)
+    ref = -0.5 * y.T @ y
+    il, iu = np.tril_indices(n), np.triu_indices(n, 1)
+    assert np.allclose(got[il], ref[il], rtol=0, atol=4 * n * EPS * (np.abs(y.T) @ np.abs(y)).max())
+    np.testing.assert_array_equal(got[iu], c0[iu])
+
+
+@pytest.mark.parametrize("n", [1, 40, 64, 65, 130, 300, 700])
+def test_trtri_vs_numpy(h, n):
+    """Y = L^{-1} by the recursive blocked inverse (diagonal 64-blocks inverted in one kernel,
+    off-diagonal blocks Y21 = -Y22 L21 Y11 with both triangular skips); the upper triangle of
+    the input is ignored and that of Y is zero.  Tolerance: forward error of a triangular
+    inverse, <= c * n * eps * cond(L) relative to |L^{-1}|."""
+    rng = np.random.default_rng(n + 11)
+    x = rng.standard_normal((n + 3, n))
+    l_true = np.linalg.cholesky(x.T @ x + n * np.eye(n))
+    l_in = l_true + np.triu(rng.standard_normal((n, n)), 1)  # garbage above the diagonal
+    dl, dy = dev(l_in), dev(rng.standard_normal((n, n)))
+    assert zb.lib().zolo_dtrtri_dev(h.ptr, n, dl.data_ptr(), n, dy.data_ptr(), n) == 0
+    got = host(dy)
+    ref = np.linalg.inv(l_true)
+    cond = np.linalg.cond(l_true)
+    assert np.count_nonzero(np.triu(got, 1)) == 0
+    assert np.linalg.norm(got - ref) <= 10 * n * EPS * cond * np.linalg.norm(ref)
+    assert np.linalg.norm(got @ l_true - np.eye(n)) <= 10 * n * EPS * cond
+    assert zb.lib().zolo_dtrtri_dev(h.ptr, -1, dl.data_ptr(), n, dy.data_ptr(), n) == -2
+
+
 def test_dgemm_split_k(h):
     """Small output with a long reduction takes the split-K path (deterministic partial sums)."""
     rng = np.random.default_rng(3)

@@ -168,6 +168,28 @@ def test_ns_finish_matches_reference_rule(m, n, kappa, rk):
     assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
 
 
+@pytest.mark.parametrize("m,n,kappa,rk", [(300, 300, 1e12, 8), (420, 250, 1e10, 4), (129, 129, 1e16, 8),
+                                          (700, 700, 1e14, 8), (65, 65, 1e8, 3)])
+def test_chol_inverse_matches_solve_form(m, n, kappa, rk):
+    """Cholesky iterations through S = sum_j w_j L_j^{-T} L_j^{-1} and one Z = X S against the
+    two-triangular-solve form (zolochol.f90:87-113): same branch sequence, both backward
+    stable (10*n*eps), the same iterate to within kappa*eps."""
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a, u, v = zo.make_matrix(n, s, 800 + m + n + rk, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)
+    q0, h0, st0 = _pzolopd1_dev_run(h, a, rk, al, be, 0)
+    h.set_option(zb.OPT_CHOL_INVERSE, 1)
+    q1, h1, st1 = _pzolopd1_dev_run(h, a, rk, al, be, 0)
+    h.set_option(zb.OPT_CHOL_INVERSE, 0)
+    h.close()
+    assert st1["branches"] == st0["branches"] and "CH" in st1["branches"]
+    check_pd(a, q1, h1, n)
+    assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
+    assert np.linalg.norm(q1 - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
+
+
 def test_solves_are_bitwise_reproducible():
     """Fixed reduction orders everywhere (no floating-point atomics): the same
     solve twice gives the same bits, for both Zolo-PD forms and QDWH."""

@@ -112,6 +112,7 @@ _SIGS = [
     ("zolo_dpotrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
     ("zolo_dtrsm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                  C.c_int64, C.c_void_p, C.c_int64]),
+    ("zolo_dtrtri_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64]),
     ("zolo_dgeqrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                   C.c_void_p]),
     ("zolo_dorgqr_dev", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
@@ -134,6 +135,7 @@ _SIGS = [
 
 OPT_SHARED_QR = 1
 OPT_NS_FINISH = 2
+OPT_CHOL_INVERSE = 3
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]

@@ -3,6 +3,7 @@
 // hot path.  See include/zolo_b200.h for the contract of every symbol.
 #include "../../include/zolo_b200.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -228,6 +229,10 @@ int zolo_set_option(zolo_handle_t h, int option, int value) {
     }
     if (option == ZOLO_OPT_NS_FINISH) {
       c.zolo_ns_finish = value != 0;
+      return 0;
+    }
+    if (option == ZOLO_OPT_CHOL_INVERSE) {
+      c.zolo_chol_inverse = value != 0;
       return 0;
     }
     return -1;
@@ -506,6 +511,21 @@ int zolo_dtrsm_dev(zolo_handle_t h, char trans, int m, int n, const double* dL, 
     zolo::diag_inverses(c, n, L, 1, D);
     if (upper(trans)) zolo::trsm_rlt(c, m, n, L, X, Y, 1, D);
     else zolo::trsm_rln(c, m, n, L, X, Y, 1, D);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    return 0;
+  });
+}
+
+int zolo_dtrtri_dev(zolo_handle_t h, int n, const double* dL, int64_t ldl, double* dY, int64_t ldy) {
+  if (n < 0) return -2;
+  if (ldl < std::max(1, n)) return -4;
+  if (ldy < std::max(1, n)) return -6;
+  if (n == 0) return 0;
+  return guarded(h, [&](Context& c) {
+    zolo::Mat L{const_cast<double*>(dL), ldl, 0}, Y{dY, ldy, 0};
+    zolo::DiagInv D{c.buf("dinv", static_cast<size_t>(zolo::nblocks(n)) * 4096), 0};
+    zolo::diag_inverses(c, n, L, 1, D);
+    zolo::trtri_lower(c, n, L, Y, 1, D);
     zolo::ck(cudaStreamSynchronize(c.stream()));
     return 0;
   });

@@ -88,6 +88,9 @@ class Context {
   int zolo_shared_qr = 1;
   // Zolo-PD stopping: 0 = reference rule, 1 = Newton-Schulz finish once ||X^T X - I|| is small.
   int zolo_ns_finish = 0;
+  // Zolo-PD Cholesky iterations: 0 = two triangular solves per term (zolochol.f90),
+  // 1 = explicit inverses summed into S, then one Z = X S.
+  int zolo_chol_inverse = 0;
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles

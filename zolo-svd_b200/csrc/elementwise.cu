@@ -207,6 +207,16 @@ __global__ void ns_prepare_kernel(int n, double* G, int64_t ldg, int write, doub
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// B(j, i) = B(i, j) for i > j: the lower triangle copied to the upper one
+__global__ void mirror_lower_kernel(int n, double* B, int64_t ldb) {
+  const int64_t total = static_cast<int64_t>(n) * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n), j = static_cast<int>(e / n);
+    if (i > j) B[j + static_cast<int64_t>(i) * ldb] = B[i + static_cast<int64_t>(j) * ldb];
+  }
+}
+
 __global__ void set_identity_kernel(int m, int n, double* Q, int64_t ldq, int64_t strideQ, double diag) {
   double* Qb = Q + blockIdx.y * strideQ;
   const int64_t total = static_cast<int64_t>(m) * n;
@@ -363,6 +373,12 @@ cudaError_t ns_prepare(int n, double* G, int64_t ldg, double* partial, double* e
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return reduce_sum(partial, blocks, err2, st);
+}
+
+cudaError_t mirror_lower(int n, double* B, int64_t ldb, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  mirror_lower_kernel<<<grid_for(static_cast<int64_t>(n) * n), TPB, 0, st>>>(n, B, ldb);
+  return cudaGetLastError();
 }
 
 cudaError_t set_identity(int m, int n, double* Q, int64_t ldq, int64_t strideQ, int batch, double diag,

@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(NT, C::MINB) dgemm_kernel(KParams kp) {
   const int M = p.M, N = p.N;
 
   int kb = 0, ke = p.K;
-  if (p.kfrom_n) kb = min(n0 / BK * BK, ke);
+  if (p.kfrom_n) kb = min((p.kfrom_n == 2 ? m0 : n0) / BK * BK, ke);
+  if (p.kto_m) ke = max(kb, min(ke, m0 + BM));
   if (kp.splitk > 1) {
     const int span = ke - kb;
     int len = (span + kp.splitk - 1) / kp.splitk;
@@ -460,7 +461,8 @@ cudaError_t dgemm(GemmArgs a, const Scratch& ws, cudaStream_t st) {
       kp.P = ws.ptr;
     }
   }
-  kp.preload = (kp.splitk <= 1 && a.beta != 0.0 && !a.tri && !a.alpha_vec && (a.alpha == 1.0 || a.alpha == -1.0) &&
+  kp.preload = (kp.splitk <= 1 && a.beta != 0.0 && !a.tri && !a.kto_m && !a.alpha_vec &&
+                 (a.alpha == 1.0 || a.alpha == -1.0) &&
                 a.K <= 64)
                    ? 1
                    : 0;

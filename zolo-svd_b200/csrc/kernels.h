@@ -21,7 +21,9 @@ struct GemmArgs {
   const double* alpha_vec = nullptr;  // per-batch factor a_b (device), nullptr = 1
   int batch = 1;
   int tri = 0;      // 1: M == N, write only C(i,j) with i >= j (lower triangle)
-  int kfrom_n = 0;  // 1: op(B)(k,n) == 0 for k < n (op(B) lower triangular): skip those k
+  int kfrom_n = 0;  // 1: op(B)(k,n) == 0 for k < n (op(B) lower triangular): skip those k;
+                    // 2: op(A)(m,k) == 0 for k < m (op(A) upper triangular): skip those k
+  int kto_m = 0;    // 1: op(A)(m,k) == 0 for k > m (op(A) lower triangular): skip those k
   int splitk = 0;   // 0 = choose; 1 = off; >1 = number of K slices
 };
 
@@ -74,6 +76,8 @@ cudaError_t transpose(int m, int n, const double* A, int64_t lda, double* B, int
 // (3I - G)/2, both triangles; always *err2 = ||G_in - I||_F^2 (partial: >= 1024
 // doubles of scratch).
 cudaError_t ns_prepare(int n, double* G, int64_t ldg, double* partial, double* err2, int write, cudaStream_t st);
+// B's upper triangle = its lower triangle mirrored (B n x n)
+cudaError_t mirror_lower(int n, double* B, int64_t ldb, cudaStream_t st);
 cudaError_t set_identity(int m, int n, double* Q, int64_t ldq, int64_t strideQ, int batch,
                          double diag, cudaStream_t st);
 // A(i,i) += d

@@ -19,7 +19,7 @@ int split_point(int n) {
 }  // namespace
 
 void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
-          int batch, const double* alpha_vec, int tri, int kfrom_n, cudaStream_t st) {
+          int batch, const double* alpha_vec, int tri, int kfrom_n, cudaStream_t st, int kto_m) {
   GemmArgs a;
   a.M = M;
   a.N = N;
@@ -41,6 +41,7 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   a.batch = batch;
   a.tri = tri;
   a.kfrom_n = kfrom_n;
+  a.kto_m = kto_m;
   const size_t need = dgemm_splitk_bytes(a, num_sms());
   if (need) c.ensure_splitk(need);
   cudaStream_t s = st ? st : c.stream();
@@ -49,9 +50,18 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   if (c.prof.on) {
     // algorithmic flops: lower triangle only (tri); k >= output column (kfrom_n)
     double f = (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K;
-    if (kfrom_n) {
+    if (kfrom_n == 2) {
+      // row i uses k >= i, over its lower-triangle (tri) or all N columns
+      f = 0.0;
+      for (int i = 0; i < std::min(M, K); ++i) f += 2.0 * (tri ? std::min(i + 1, N) : N) * (K - i);
+    } else if (kfrom_n) {
       const double nn = std::min(N, K);
       f = 2.0 * M * (static_cast<double>(N) * K - nn * (nn - 1.0) / 2.0 - (N - nn) * static_cast<double>(K));
+    }
+    if (kto_m) {
+      // row i uses k <= i: sum over rows of min(K, i + 1)
+      const double mm = std::min(M, K);
+      f = 2.0 * N * (mm * (mm + 1.0) / 2.0 + (M - mm) * static_cast<double>(K));
     }
     c.prof.begin(cls, f * batch, s, &rec);
   }
@@ -127,6 +137,28 @@ struct PanelRows {
   int mp, split;
   int64_t gap;
 };
+
+static void trtri_rec(Context& c, int n, Mat L, Mat Y, int batch, DiagInv D, int k0, Mat Tmp) {
+  if (n <= NB) {
+    ck(scale_copy(n, n, 1.0, D.block(k0), NB, D.stride, Y.p, Y.ld, Y.stride, batch, 0.0, c.stream()));
+    c.stats.launches++;
+    return;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  trtri_rec(c, n1, L, Y, batch, D, k0, Tmp);
+  trtri_rec(c, n2, L.at(n1, n1), Y.at(n1, n1), batch, D, k0 + n1 / NB, Tmp);
+  // Y21 = -Y22 (L21 Y11): Y11 lower (k from the output column), Y22 lower (k up to the row)
+  gemm(c, 0, 0, n2, n1, n1, 1.0, L.at(n1, 0), Y, 0.0, Tmp, batch, nullptr, 0, 1);
+  gemm(c, 0, 0, n2, n1, n2, -1.0, Y.at(n1, n1), Tmp, 0.0, Y.at(n1, 0), batch, nullptr, 0, 0, nullptr, 1);
+}
+
+void trtri_lower(Context& c, int n, Mat L, Mat Y, int batch, DiagInv D) {
+  ck(set_identity(n, n, Y.p, Y.ld, Y.stride, batch, 0.0, c.stream()));  // zero upper triangle
+  c.stats.launches++;
+  const int64_t ldt = (n + 1) / 2 * 2;
+  Mat Tmp{c.buf("trtri_tmp", static_cast<size_t>(ldt) * n * batch), ldt, ldt * n};
+  trtri_rec(c, n, L, Y, batch, D, 0, Tmp);
+}
 
 static inline PanelRows panel_rows(int mtot, int m_top, bool top_tri, int j, int jb) {
   const int hi = m_top >= 0 ? std::min(mtot, m_top + j + jb) : mtot;

@@ -28,8 +28,7 @@ inline int nblocks(int n) { return (n + kLeaf - 1) / kLeaf; }
 
 void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
           int batch, const double* alpha_vec = nullptr, int tri = 0, int kfrom_n = 0,
-          cudaStream_t st = nullptr);
-
+          cudaStream_t st = nullptr, int kto_m = 0);
 // Lower Cholesky in place (n x n), recursive; info[b] > 0 on failure (LAPACK convention).
 // Dinv receives the inverses of the diagonal blocks of L (used by the solves below).
 void potrf(Context& c, int n, Mat A, int batch, int* dinfo, DiagInv Dinv);
@@ -39,6 +38,10 @@ void diag_inverses(Context& c, int n, Mat L, int batch, DiagInv Dinv);
 void trsm_rlt(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv Dinv, int k0 = 0);
 // Y = X L^{-1}
 void trsm_rln(Context& c, int m, int n, Mat L, Mat X, Mat Y, int batch, DiagInv Dinv, int k0 = 0);
+// Y = L^{-1} (lower triangular; Y's strictly upper triangle is set to zero), recursively:
+// Y21 = -Y22 (L21 Y11), each product skipping the zero triangle of its triangular
+// operand (n^3/3 flops); the 64 x 64 diagonal blocks are Dinv's.
+void trtri_lower(Context& c, int n, Mat L, Mat Y, int batch, DiagInv Dinv);
 
 // Householder QR (in place, panels of 32) of the mtot x n matrices W.  With
 // `m_top` >= 0 the matrix is the stack [X (m_top rows); D] where D is upper

@@ -414,6 +414,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     double maxc = coeff[0];
     for (int i = 1; i < 2 * rk; ++i) maxc = std::max(maxc, coeff[i]);
     bool use_qr = (it == 0 || con > 1.0e3) && maxc > 3.0e2;
+    bool z_summed = false;  // Z holds sum_j w_j Z_j / FONE already (one Z instead of r)
     if (!use_qr) {
       gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       if (ns_finish) {
@@ -438,6 +439,26 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       if (pinfo != 0) {
         if (c.stats.info == 0) c.stats.info = pinfo;
         use_qr = true;  // fall back to the QR form for this step
+      } else if (c.zolo_chol_inverse && !left) {
+        // explicit form: S = sum_b w_b W_b^{-1}, W_b^{-1} = L_b^{-T} L_b^{-1}, then one Z = X S
+        const double fone_c = zolo_fone(coeff.data(), rk);
+        Mat Y{c.buf("zc_y", static_cast<size_t>(ldn) * n * rk), ldn, ldn * n};
+        trtri_lower(c, n, Wc, Y, rk, Dz);
+        Mat S{c.buf("zc_s", static_cast<size_t>(ldn) * n), ldn, 0};
+        for (int b = 0; b < rk; ++b) {
+          const double w = -coeff[2 * rk + b] / fone_c;
+          gemm(c, 1, 0, n, n, n, w, Mat{Y.p + b * Y.stride, ldn, 0}, Mat{Y.p + b * Y.stride, ldn, 0},
+               b == 0 ? 0.0 : 1.0, S, 1, nullptr, 1, 2);
+        }
+        ck(mirror_lower(n, S.p, S.ld, c.stream()));
+        c.stats.launches++;
+        gemm(c, 0, 0, m, n, n, 1.0, Mat{X, ldx, 0}, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
+        z_summed = true;
+        c.stats.chol_iterations++;
+        if (it < 16) c.stats.branch[it] = 2;
+        const double dm = m, dn = n;
+        c.stats.flops += dm * dn * dn + rk * (dn * dn * dn / 3.0 + 2.0 * dm * dn * dn);
+        c.stats.flops_exec_delta += rk * (dn * dn * dn - 2.0 * dm * dn * dn) + 2.0 * dm * dn * dn;
       } else {
         spd_solve(c, m, n, X, ldx, Wc, Dz, Z, rk, left);
         for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b];
@@ -449,9 +470,9 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     }
     const double fone = zolo_fone(coeff.data(), rk);
     const double con_next = zolo_next_con(con, coeff.data(), rk, fone);
-    bool shared = false;
     if (use_qr) {
-      shared = c.zolo_shared_qr != 0;
+      const bool shared = c.zolo_shared_qr != 0;
+      z_summed = shared;
       // the first iteration may reuse the QR of A/alpha: X0 = (A/alpha)/beta
       const Prefactored* pfi = (shared && it == 0) ? pf : nullptr;
       for (int b = 0; b < rk; ++b) hv[b] = std::sqrt(coeff[2 * b]) * (pfi ? beta : 1.0);
@@ -472,8 +493,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       c.stats.qr_iterations++;
       if (it < 16) c.stats.branch[it] = 1;
     }
-    if (shared) {
-      // Z already holds sum_j w_j Q1_j Q2_j^T / FONE
+    if (z_summed) {
+      // Z already holds sum_j w_j Z_j / FONE
       ck(combine_update(m, n, X, ldx, Z.p, Z.ld, 0, 1, 1.0 / fone, 1.0, nullptr, part, scal, c.stream()));
     } else {
       for (int b = 0; b < rk; ++b) hv[16 + b] /= fone;

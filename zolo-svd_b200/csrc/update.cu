@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(UT, 2) rank_update_kernel(UpdParams p) {
 }  // namespace
 
 bool rank_update_applies(const GemmArgs& a) {
-  return !a.transA && !a.transB && a.K >= 1 && a.K <= UK && !a.tri && !a.kfrom_n && !a.alpha_vec &&
+  return !a.transA && !a.transB && a.K >= 1 && a.K <= UK && !a.tri && !a.kfrom_n && !a.kto_m && !a.alpha_vec &&
          static_cast<int64_t>(a.M) * a.N >= static_cast<int64_t>(UM) * UN * 16;
 }
 
