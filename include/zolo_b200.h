@@ -110,6 +110,14 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * are well conditioned in the Cholesky iterations (condition <= CON^2, CON <= 1e3), so
  * both forms agree to rounding.  SYM = 'S' keeps the solves.  No reference counterpart. */
 #define ZOLO_OPT_CHOL_INVERSE 3
+/* ZOLO_OPT_BETA_FROB: 0 (default) = zolo_polar_dev takes beta = 1/(sqrt(n) ||R^{-1}||_1)
+ * (zolo_bounds_dev mode 1, the reference driver's estimate); 1 = beta = 1/||R^{-1}||_F (mode 2),
+ * also a lower bound on sigma_min but up to sqrt(n) times tighter.  The Zolotarev
+ * coefficients (Auxil_Zolo.f90:165-200, alpha = acos(1/CON)) lose their accuracy once
+ * CON = 1/beta passes about 1e15, after which the second iteration no longer converges and
+ * one more is needed; the tighter beta keeps CON below that for condition numbers up to
+ * about 1e13.  No reference counterpart. */
+#define ZOLO_OPT_BETA_FROB 4
 int zolo_set_option(zolo_handle_t handle, int option, int value);
 
 /* ---- host scalar routines (no GPU needed) ---- */
@@ -207,7 +215,8 @@ int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double al
                       int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh);
 /* The driver's bounds (test_zolodrv1.f90:167-189 replaced by a QR + R^{-1} estimate):
  * alpha = ||A||_F, beta = 1/(sqrt(n) ||R^{-1}||_1) for A/alpha = QR (mode 1) or
- * ||A/alpha||_1 / (sqrt(n) ||R^{-1}||_1) (mode 0). */
+ * ||A/alpha||_1 / (sqrt(n) ||R^{-1}||_1) (mode 0), or 1/||R^{-1}||_F (mode 2: still a
+ * lower bound on sigma_min(A/alpha), and never below mode 1's).  Returns -7 for another mode. */
 int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* dA, int64_t lda, int mode,
                     double* alpha, double* beta);
 /* H = (Q^T A + A^T Q)/2 (pqdwhfacs.f90:460-466, ZoloCHK1.f90:80-83). */
@@ -231,7 +240,7 @@ int zolo_zoloeig_dev(zolo_handle_t h, int n, const double* dQ, int64_t ldq, cons
 /* ---- kernel-level entry points (building blocks, used by the parity tests) ---- */
 /* C = alpha op(A) op(B) + beta C (PDGEMM on a 1x1 grid); tri = lower-triangle-only output,
  * kfrom_n = 1: op(B) is lower triangular (TRMM-like skip of k < column);
- * kfrom_n = 2: op(A) is upper triangular (skip of k < row). */
+ * kfrom_n = 2: op(A) is upper triangular (skip of k < row); kfrom_n = 3: both (k >= max(row, column)). */
 int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
                    int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
                    int kfrom_n);

@@ -157,6 +157,21 @@ def test_dgemm_row_triangular_skip(h):
     np.testing.assert_array_equal(got[iu], c0[iu])
 
 
+def test_dgemm_both_triangular_skip(h):
+    """kfrom_n = 3: op(A) upper and op(B) lower triangular, so entry (i, j) sums k >= max(i, j)
+    only (Q1 Q2^T of the shared-QR Zolotarev terms, both factors upper triangular)."""
+    rng = np.random.default_rng(5)
+    n = 301
+    q1 = np.triu(rng.standard_normal((n, n)))
+    q2 = np.triu(rng.standard_normal((n, n)))
+    d1, d2, dc = dev(q1), dev(q2), dev(rng.standard_normal((n, n)))
+    r = zb.lib().zolo_dgemm_dev(h.ptr, b"N", b"T", n, n, n, 2.0, d1.data_ptr(), n, d2.data_ptr(), n, 0.0,
+                                dc.data_ptr(), n, 0, 3)
+    assert r == 0
+    ref = 2.0 * q1 @ q2.T
+    assert np.allclose(host(dc), ref, rtol=0, atol=8 * n * EPS * (np.abs(q1) @ np.abs(q2.T)).max())
+
+
 @pytest.mark.parametrize("n", [1, 40, 64, 65, 130, 300, 700])
 def test_trtri_vs_numpy(h, n):
     """Y = L^{-1} by the recursive blocked inverse (diagonal 64-blocks inverted in one kernel,

@@ -346,3 +346,51 @@ def test_bounds_dev_matches_oracle():
     assert abs(be - be_o) <= 1e-5 * be_o
     assert be <= s[-1] / al * (1 + 1e-8)  # a true lower bound on sigma_min(A/alpha)
     h.close()
+
+
+@pytest.mark.parametrize("m,n,kappa", [(120, 120, 1e9), (300, 200, 1e14), (257, 257, 1e3)])
+def test_bounds_frobenius_mode(m, n, kappa):
+    """Mode 2: beta = 1/||R^{-1}||_F, a lower bound on sigma_min(A/alpha) that is never below
+    mode 1's 1/(sqrt(n) ||R^{-1}||_1); a bad mode is rejected."""
+    s = np.geomspace(1, 1.0 / kappa, n)
+    a, _, _ = zo.make_matrix(n, s, 78 + m, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    al, be1, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)
+    al2, be2, info = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=2)
+    assert info == 0 and al2 == al
+    r = np.linalg.qr(a / al, mode="r")
+    ref = 1.0 / np.linalg.norm(np.linalg.inv(r))
+    assert abs(be2 - ref) <= max(1e-10, 100 * n * EPS * kappa) * ref
+    assert be1 * (1 - 1e-8) <= be2 <= s[-1] / al * (1 + 1e-8)
+    with pytest.raises(zb.ZoloError):
+        zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=3)
+    h.close()
+
+
+@pytest.mark.parametrize("m,n,kappa", [(300, 300, 1e12), (400, 260, 1e15), (129, 129, 1e6)])
+def test_polar_dev_frobenius_beta(m, n, kappa):
+    """zolo_polar_dev with ZOLO_OPT_BETA_FROB: beta from mode 2, no more iterations than with
+    the reference driver's beta, and the same polar factor (10 n eps; Q within kappa eps)."""
+    import torch
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a, u, v = zo.make_matrix(n, s, 650 + m + n, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    out = {}
+    for frob in (0, 1):
+        h.set_option(zb.OPT_BETA_FROB, frob)
+        dq = torch.zeros_like(da)
+        dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n) == 0
+        out[frob] = (zb.device_to_colmajor(dq), zb.device_to_colmajor(dh), h.stats())
+    _, be2, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=2)
+    h.set_option(zb.OPT_BETA_FROB, 0)
+    h.close()
+    (q0, h0, st0), (q1, h1, st1) = out[0], out[1]
+    assert st1["beta"] == be2 and st1["beta"] >= st0["beta"]
+    assert st1["iterations"] <= st0["iterations"]
+    check_pd(a, q1, h1, n)
+    assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= max(1e-12, 10 * n * EPS * kappa)
+    assert np.linalg.norm(q1 - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)

@@ -136,6 +136,7 @@ _SIGS = [
 OPT_SHARED_QR = 1
 OPT_NS_FINISH = 2
 OPT_CHOL_INVERSE = 3
+OPT_BETA_FROB = 4
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]

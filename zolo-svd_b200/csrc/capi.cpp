@@ -235,6 +235,10 @@ int zolo_set_option(zolo_handle_t h, int option, int value) {
       c.zolo_chol_inverse = value != 0;
       return 0;
     }
+    if (option == ZOLO_OPT_BETA_FROB) {
+      c.zolo_beta_frob = value != 0;
+      return 0;
+    }
     return -1;
   });
 }
@@ -393,9 +397,10 @@ int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double al
 int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* dA, int64_t lda, int mode,
                     double* alpha, double* beta) {
   if (m < n) return -2;
+  if (mode < 0 || mode > 2) return -7;
   return guarded(h, [&](Context& c) {
     c.stats = zolo::Stats{};
-    return zolo::bounds(c, m, n, sigma, dA, lda, mode ? zolo::BOUNDS_ZOLOPD : zolo::BOUNDS_PQDWHFACS, alpha, beta);
+    return zolo::bounds(c, m, n, sigma, dA, lda, static_cast<zolo::BoundsMode>(mode), alpha, beta);
   });
 }
 

@@ -30,7 +30,9 @@ void Context::release_all() {
   for (auto& kv : bufs_) cudaFree(kv.second.first);
   bufs_.clear();
   if (splitk_.ptr) cudaFree(splitk_.ptr);
+  if (splitk_side_.ptr) cudaFree(splitk_side_.ptr);
   splitk_ = Scratch{};
+  splitk_side_ = Scratch{};
 }
 
 static void* grow(std::map<std::string, std::pair<void*, size_t>>& bufs, const std::string& name, size_t bytes,
@@ -58,18 +60,20 @@ int* Context::ibuf(const std::string& name, size_t elems) {
   return static_cast<int*>(grow(bufs_, name, elems * sizeof(int), stream_));
 }
 
-void Context::ensure_splitk(size_t bytes) {
-  if (splitk_.bytes >= bytes) return;
-  if (splitk_.ptr) {
+void Context::ensure_splitk(size_t bytes, bool side) {
+  Scratch& s = side ? splitk_side_ : splitk_;
+  if (s.bytes >= bytes) return;
+  if (s.ptr) {
     ck(cudaStreamSynchronize(stream_));
-    ck(cudaFree(splitk_.ptr));
+    ck(cudaStreamSynchronize(side_));
+    ck(cudaFree(s.ptr));
   }
-  splitk_.ptr = nullptr;
-  splitk_.bytes = 0;
+  s.ptr = nullptr;
+  s.bytes = 0;
   void* p = nullptr;
   ck(cudaMalloc(&p, bytes));
-  splitk_.ptr = static_cast<double*>(p);
-  splitk_.bytes = bytes;
+  s.ptr = static_cast<double*>(p);
+  s.bytes = bytes;
 }
 
 cudaEvent_t Profiler::take() {

@@ -76,8 +76,9 @@ class Context {
   // Named cached device buffer of at least `elems` doubles (grow-only).
   double* buf(const std::string& name, size_t elems);
   int* ibuf(const std::string& name, size_t elems);
-  Scratch& splitk() { return splitk_; }
-  void ensure_splitk(size_t bytes);
+  // split-K partial sums; GEMMs on the side stream have their own
+  Scratch& splitk(bool side = false) { return side ? splitk_side_ : splitk_; }
+  void ensure_splitk(size_t bytes, bool side = false);
   void release_all();
 
   Stats stats;
@@ -91,6 +92,8 @@ class Context {
   // Zolo-PD Cholesky iterations: 0 = two triangular solves per term (zolochol.f90),
   // 1 = explicit inverses summed into S, then one Z = X S.
   int zolo_chol_inverse = 0;
+  // zolo_polar's bounds: 0 = beta = 1/(sqrt(n) ||R^-1||_1) (test_zolodrv1.f90), 1 = 1/||R^-1||_F.
+  int zolo_beta_frob = 0;
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles
@@ -102,7 +105,7 @@ class Context {
   cudaStream_t stream_ = nullptr, own_stream_ = nullptr, side_ = nullptr;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   std::map<std::string, std::pair<void*, size_t>> bufs_;
-  Scratch splitk_;
+  Scratch splitk_, splitk_side_;
 };
 
 }  // namespace zolo

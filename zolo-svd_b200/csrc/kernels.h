@@ -22,7 +22,8 @@ struct GemmArgs {
   int batch = 1;
   int tri = 0;      // 1: M == N, write only C(i,j) with i >= j (lower triangle)
   int kfrom_n = 0;  // 1: op(B)(k,n) == 0 for k < n (op(B) lower triangular): skip those k;
-                    // 2: op(A)(m,k) == 0 for k < m (op(A) upper triangular): skip those k
+                    // 2: op(A)(m,k) == 0 for k < m (op(A) upper triangular): skip those k;
+                    // 3: both (k from max(row, column))
   int kto_m = 0;    // 1: op(A)(m,k) == 0 for k > m (op(A) lower triangular): skip those k
   int splitk = 0;   // 0 = choose; 1 = off; >1 = number of K slices
 };
@@ -98,7 +99,7 @@ cudaError_t trtri_blocks(int n, const double* L, int64_t ldl, int64_t strideL, d
 
 // ---- Householder QR panel (qr.cu) ----
 // Factor the m x w panel of each batch entry (w <= 32) in place: V below the
-// diagonal (unit diagonal implied), R on/above it, tau[w], T (w x w upper, ldt = w)
+// diagonal (unit diagonal implied), R on/above it, tau[w], T (w x w upper, ld 32)
 // of the compact WY form I - V T V^T.  Vexp receives V explicitly (m x w, ldv).
 // Row gap: with split > 0, logical row r >= split of the panel is the physical
 // row r + gap of A (two row segments; Vexp stays in logical rows).
@@ -112,7 +113,11 @@ int qr_panel_config(int m, int w);
 cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t strideA, double* V,
                       int64_t ldv, int64_t strideV, int batch, cudaStream_t st, int split = 0,
                       int64_t gap = 0);
-// P'(b) = T(b)^T * P(b) (trans=1) or T(b) * P(b) (trans=0); T w x w upper (ldt=w), P w x n.
+// TB(b) (jb x jb, ld ldtb) <- block diagonal of the ceil(jb/32) consecutive 32 x 32 panel T
+// factors at T + b*strideT (ld 32, 1024 apart), zero elsewhere.
+cudaError_t block_t_init(int jb, const double* T, int64_t strideT, double* TB, int64_t ldtb, int64_t strideTB,
+                         int batch, cudaStream_t st);
+// P'(b) = T(b)^T * P(b) (trans=1) or T(b) * P(b) (trans=0); T w x w upper (ld 32), P w x n.
 cudaError_t apply_t(int w, int n, const double* T, int64_t strideT, double* P, int64_t ldp,
                     int64_t strideP, int trans, int batch, cudaStream_t st);
 

@@ -9,6 +9,7 @@ namespace zolo {
 namespace {
 constexpr int NB = kLeaf;  // leaf of the Cholesky / TRSM recursion
 constexpr int PW = 32;     // Householder panel width
+constexpr int QB = 128;    // Householder block: four panels, one rank-128 trailing update
 
 int split_point(int n) {
   int n1 = ((n / 2) + NB - 1) / NB * NB;
@@ -43,8 +44,9 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   a.kfrom_n = kfrom_n;
   a.kto_m = kto_m;
   const size_t need = dgemm_splitk_bytes(a, num_sms());
-  if (need) c.ensure_splitk(need);
   cudaStream_t s = st ? st : c.stream();
+  const bool side = s == c.side_stream() && s != c.stream();
+  if (need) c.ensure_splitk(need, side);
   Profiler::Rec rec;
   const int cls = tri ? 6 : (M <= 32 ? 3 : (N <= 64 ? 4 : (K <= 64 ? 5 : 0)));
   if (c.prof.on) {
@@ -54,6 +56,14 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
       // row i uses k >= i, over its lower-triangle (tri) or all N columns
       f = 0.0;
       for (int i = 0; i < std::min(M, K); ++i) f += 2.0 * (tri ? std::min(i + 1, N) : N) * (K - i);
+    } else if (kfrom_n == 3) {
+      // entry (i, j) uses k >= max(i, j) (no tri)
+      f = 0.0;
+      for (int i = 0; i < std::min(M, K); ++i) {
+        const double jn = std::min(i + 1, N);  // columns j <= i: K - i each
+        const double jm = std::max(0, std::min(N, K) - i - 1);  // columns i < j < K: K - j each
+        f += 2.0 * (jn * (K - i) + jm * (K - i - 1) - jm * (jm - 1.0) / 2.0);
+      }
     } else if (kfrom_n) {
       const double nn = std::min(N, K);
       f = 2.0 * M * (static_cast<double>(N) * K - nn * (nn - 1.0) / 2.0 - (N - nn) * static_cast<double>(K));
@@ -65,7 +75,7 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
     }
     c.prof.begin(cls, f * batch, s, &rec);
   }
-  ck(dgemm(a, c.splitk(), s));
+  ck(dgemm(a, c.splitk(side), s));
   if (c.prof.on) c.prof.end(rec, s);
   c.stats.launches += need ? 2 : 1;
 }
@@ -166,91 +176,134 @@ static inline PanelRows panel_rows(int mtot, int m_top, bool top_tri, int j, int
   return PanelRows{jb + (hi - m_top), jb, static_cast<int64_t>(m_top) - j - jb};
 }
 
-// P = V^T B over the panel rows (B starts at the panel's first row)
-static void panel_vt_b(Context& c, const PanelRows& R, int jb, int ncols, Mat V, Mat B, Mat P, int batch) {
-  gemm(c, 1, 0, jb, ncols, R.split, 1.0, V, B, 0.0, P, batch);
+// P = V^T B over the panel rows (B starts at the panel's first row; V holds the rows packed)
+static void panel_vt_b(Context& c, const PanelRows& R, int jb, int ncols, Mat V, Mat B, Mat P, int batch,
+                       cudaStream_t st = nullptr) {
+  gemm(c, 1, 0, jb, ncols, R.split, 1.0, V, B, 0.0, P, batch, nullptr, 0, 0, st);
   if (R.split < R.mp)
     gemm(c, 1, 0, jb, ncols, R.mp - R.split, 1.0, V.at(R.split, 0), B.at(static_cast<int>(R.split + R.gap), 0),
-         1.0, P, batch);
+         1.0, P, batch, nullptr, 0, 0, st);
 }
 
 // B -= V P over the panel rows
-static void panel_b_minus_vp(Context& c, const PanelRows& R, int jb, int ncols, Mat V, Mat P, Mat B, int batch) {
-  gemm(c, 0, 0, R.split, ncols, jb, -1.0, V, P, 1.0, B, batch);
+static void panel_b_minus_vp(Context& c, const PanelRows& R, int jb, int ncols, Mat V, Mat P, Mat B, int batch,
+                             cudaStream_t st = nullptr) {
+  gemm(c, 0, 0, R.split, ncols, jb, -1.0, V, P, 1.0, B, batch, nullptr, 0, 0, st);
   if (R.split < R.mp)
     gemm(c, 0, 0, R.mp - R.split, ncols, jb, -1.0, V.at(R.split, 0), P, 1.0,
-         B.at(static_cast<int>(R.split + R.gap), 0), batch);
+         B.at(static_cast<int>(R.split + R.gap), 0), batch, nullptr, 0, 0, st);
 }
 
+// T_B (jb x jb upper) of the block reflector I - V_B T_B V_B^T = H_1 H_2 ... of the block's
+// 32-column panels (the compact WY recursion of LAPACK DLARFT, by panels): the diagonal
+// blocks are the panels' T, and T_B(0:c0, q) = -T_B(0:c0, 0:c0) (V_B(:, 0:c0)^T V_q) T_q.
+// VB: the block's explicit V, mp packed rows.  T: the first panel's T (32 x 32 per panel).
+static void block_t(Context& c, int jb, Mat VB, int mp, const double* T, int64_t strideT, Mat TB, int batch) {
+  Mat G{c.buf("qr_bg", static_cast<size_t>(QB) * QB * batch), QB, static_cast<int64_t>(QB) * QB};
+  Mat Tmp{c.buf("qr_btmp", static_cast<size_t>(QB) * PW * batch), QB, static_cast<int64_t>(QB) * PW};
+  // lower triangle of V_B^T V_B: its transpose gives the blocks above the diagonal
+  gemm(c, 1, 0, jb, jb, mp, 1.0, VB, VB, 0.0, G, batch, nullptr, 1, 0);
+  ck(block_t_init(jb, T, strideT, TB.p, TB.ld, TB.stride, batch, c.stream()));
+  c.stats.launches++;
+  for (int c0 = PW; c0 < jb; c0 += PW) {
+    const int w = std::min(PW, jb - c0);
+    // Tmp = T_B(0:c0, 0:c0) G(c0:c0+w, 0:c0)^T  (T_B upper: k from the row)
+    gemm(c, 0, 1, c0, w, c0, 1.0, TB, G.at(c0, 0), 0.0, Tmp, batch, nullptr, 0, 2);
+    gemm(c, 0, 0, c0, w, w, -1.0, Tmp, TB.at(c0, c0), 0.0, TB.at(0, c0), batch);
+  }
+}
+
+// Householder QR in 128-column blocks of four 32-column panels.  Inside a block each panel
+// updates only the block's remaining columns (rank-32); the trailing columns take one
+// rank-128 update per block, C -= V_B (T_B^T (V_B^T C)), whose GEMMs have K = rows and
+// K = 128.  Look-ahead: the next block's columns are updated first, then the next block is
+// factored on the side stream while the main stream updates the rest.
 void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T, int batch, bool top_tri) {
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
-  // explicit V of consecutive panels alternates between two buffers (look-ahead)
-  double* vb = c.buf("qr_v2", static_cast<size_t>(ldv) * PW * batch * 2);
-  Mat V[2] = {Mat{vb, ldv, ldv * PW}, Mat{vb + ldv * PW * batch, ldv, ldv * PW}};
-  Mat P{c.buf("qr_p", static_cast<size_t>(PW) * n * batch), PW, static_cast<int64_t>(PW) * n};
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
+  Mat Vp{c.buf("qr_v2", static_cast<size_t>(ldv) * PW * batch), ldv, ldv * PW};
+  Mat Pp{c.buf("qr_p", static_cast<size_t>(PW) * QB * batch), PW, static_cast<int64_t>(PW) * QB};
+  Mat VB{c.buf("qr_vb", static_cast<size_t>(ldv) * QB * batch), ldv, ldv * QB};
+  Mat TB{c.buf("qr_tb", static_cast<size_t>(QB) * QB * batch), QB, static_cast<int64_t>(QB) * QB};
+  Mat WB{c.buf("qr_wb", static_cast<size_t>(QB) * n * batch), QB, static_cast<int64_t>(QB) * n};
+  Mat PB{c.buf("qr_pb", static_cast<size_t>(QB) * n * batch), QB, static_cast<int64_t>(QB) * n};
   cudaStream_t ms = c.stream(), ss = c.side_stream();
-  auto panel = [&](int pj, cudaStream_t st) {
-    const int j = pj * PW;
-    const int jb = std::min(PW, n - j);
-    const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
-    Profiler::Rec rec;
-    if (c.prof.on) c.prof.begin(1, 2.0 * R.mp * static_cast<double>(jb) * jb * batch, st, &rec);
-    ck(qr_panel(R.mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + pj * PW * PW, strideT, V[pj & 1].p,
-                V[pj & 1].ld, V[pj & 1].stride, batch, st, R.split, R.gap));
-    if (c.prof.on) c.prof.end(rec, st);
-    c.stats.launches++;
+  auto factor_block = [&](int J, cudaStream_t st) {
+    const int jend = std::min(n, J + QB);
+    for (int j = J; j < jend; j += PW) {
+      const int jb = std::min(PW, n - j);
+      const int pj = j / PW;
+      const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
+      Profiler::Rec rec;
+      if (c.prof.on) c.prof.begin(1, 2.0 * R.mp * static_cast<double>(jb) * jb * batch, st, &rec);
+      ck(qr_panel(R.mp, jb, W.at(j, j).p, W.ld, W.stride, tau + j, n, T + pj * PW * PW, strideT, Vp.p, Vp.ld,
+                  Vp.stride, batch, st, R.split, R.gap));
+      if (c.prof.on) c.prof.end(rec, st);
+      c.stats.launches++;
+      const int nc = jend - j - jb;
+      if (nc <= 0) continue;
+      panel_vt_b(c, R, jb, nc, Vp, W.at(j, j + jb), Pp, batch, st);
+      ck(apply_t(jb, nc, T + pj * PW * PW, strideT, Pp.p, Pp.ld, Pp.stride, 1, batch, st));
+      c.stats.launches++;
+      panel_b_minus_vp(c, R, jb, nc, Vp, Pp, W.at(j, j + jb), batch, st);
+    }
   };
-  panel(0, ms);
-  for (int pj = 0; pj < npan; ++pj) {
-    const int j = pj * PW;
-    const int jb = std::min(PW, n - j);
-    const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
-    const int nc = n - j - jb;
+  factor_block(0, ms);
+  for (int J = 0; J < n; J += QB) {
+    const int jbB = std::min(QB, n - J);
+    const int nc = n - J - jbB;
     if (nc <= 0) break;
-    const Mat& Vj = V[pj & 1];
-    // P = T^T V^T W_trail
-    panel_vt_b(c, R, jb, nc, Vj, W.at(j, j + jb), P, batch);
-    ck(apply_t(jb, nc, T + pj * PW * PW, strideT, P.p, P.ld, P.stride, 1, batch, ms));
+    const PanelRows R = panel_rows(mtot, m_top, top_tri, J, jbB);
+    ck(extract_v(R.mp, jbB, W.at(J, J).p, W.ld, W.stride, VB.p, VB.ld, VB.stride, batch, ms, R.split, R.gap));
     c.stats.launches++;
-    // next panel's columns first, then the panel on the side stream overlaps the rest
-    const int jb2 = std::min(PW, nc);
-    panel_b_minus_vp(c, R, jb, jb2, Vj, P, W.at(j, j + jb), batch);
-    const bool overlap = nc > jb2;
-    if (overlap) {
+    block_t(c, jbB, VB, R.mp, T + (J / PW) * PW * PW, strideT, TB, batch);
+    panel_vt_b(c, R, jbB, nc, VB, W.at(J, J + jbB), WB, batch, ms);
+    // P = T_B^T (V_B^T C): T_B^T is lower triangular (k up to the row)
+    gemm(c, 1, 0, jbB, nc, jbB, 1.0, TB, WB, 0.0, PB, batch, nullptr, 0, 0, ms, 1);
+    const int jn = std::min(QB, nc);
+    panel_b_minus_vp(c, R, jbB, jn, VB, PB, W.at(J, J + jbB), batch, ms);
+    if (nc > jn) {
       ck(cudaEventRecord(c.event(0), ms));
       ck(cudaStreamWaitEvent(ss, c.event(0), 0));
-      panel(pj + 1, ss);
+      factor_block(J + jbB, ss);
       ck(cudaEventRecord(c.event(1), ss));
-      panel_b_minus_vp(c, R, jb, nc - jb2, Vj, P.at(0, jb2), W.at(j, j + jb + jb2), batch);
+      panel_b_minus_vp(c, R, jbB, nc - jn, VB, PB.at(0, jn), W.at(J, J + jbB + jn), batch, ms);
       ck(cudaStreamWaitEvent(ms, c.event(1), 0));
     } else {
-      panel(pj + 1, ms);
+      factor_block(J + jbB, ms);
     }
   }
 }
 
+// Q = H_1 ... H_k applied to the identity, one 128-column block reflector at a time from the
+// last block: Q(rows, J:nq) -= V_B (T_B (V_B^T Q(rows, J:nq))).  Columns left of J are still
+// identity columns with their one above the block's rows, so V_B^T leaves them zero.
 void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq, bool top_tri) {
   if (nq < n) nq = n;
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
-  Mat V{c.buf("qr_v2", static_cast<size_t>(ldv) * PW * batch * 2), ldv, ldv * PW};
-  Mat P{c.buf("qr_p", static_cast<size_t>(PW) * nq * batch), PW, static_cast<int64_t>(PW) * nq};
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
+  Mat VB{c.buf("qr_vb", static_cast<size_t>(ldv) * QB * batch), ldv, ldv * QB};
+  Mat TB{c.buf("qr_tb", static_cast<size_t>(QB) * QB * batch), QB, static_cast<int64_t>(QB) * QB};
+  Mat WB{c.buf("qr_wb", static_cast<size_t>(QB) * nq * batch), QB, static_cast<int64_t>(QB) * nq};
+  Mat PB{c.buf("qr_pb", static_cast<size_t>(QB) * nq * batch), QB, static_cast<int64_t>(QB) * nq};
   ck(set_identity(mtot, nq, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
   c.stats.launches++;
-  for (int pj = npan - 1; pj >= 0; --pj) {
-    const int j = pj * PW;
-    const int jb = std::min(PW, n - j);
-    const PanelRows R = panel_rows(mtot, m_top, top_tri, j, jb);
-    const int nc = nq - j;
-    ck(extract_v(R.mp, jb, W.at(j, j).p, W.ld, W.stride, V.p, V.ld, V.stride, batch, c.stream(), R.split, R.gap));
+  const int nblk = (n + QB - 1) / QB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int J = b * QB;
+    const int jbB = std::min(QB, n - J);
+    const PanelRows R = panel_rows(mtot, m_top, top_tri, J, jbB);
+    const int nc = nq - J;
+    ck(extract_v(R.mp, jbB, W.at(J, J).p, W.ld, W.stride, VB.p, VB.ld, VB.stride, batch, c.stream(), R.split,
+                 R.gap));
     c.stats.launches++;
-    panel_vt_b(c, R, jb, nc, V, Q.at(j, j), P, batch);
-    ck(apply_t(jb, nc, T + pj * PW * PW, strideT, P.p, P.ld, P.stride, 0, batch, c.stream()));
-    c.stats.launches++;
-    panel_b_minus_vp(c, R, jb, nc, V, P, Q.at(j, j), batch);
+    block_t(c, jbB, VB, R.mp, T + (J / PW) * PW * PW, strideT, TB, batch);
+    panel_vt_b(c, R, jbB, nc, VB, Q.at(J, J), WB, batch);
+    // P = T_B (V_B^T Q): T_B is upper triangular (k from the row)
+    gemm(c, 0, 0, jbB, nc, jbB, 1.0, TB, WB, 0.0, PB, batch, nullptr, 0, 2);
+    panel_b_minus_vp(c, R, jbB, nc, VB, PB, Q.at(J, J), batch);
   }
 }
 

@@ -83,8 +83,8 @@ void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
 // interleaved order loses backward stability of the iteration), and panel j
 // touches only rows j .. j+31 of R_x and rows 0 .. j+31 of sqrt(c_j) I.
 // Result: Z(:, :, 0) = Q_x * sum_j w_j Q1'_j Q2'_j^T / FONE, w_j = hw[j].
-// Flops: QR of X 4mn^2 - 4n^3/3, per term 4n^3/3 (structured QR and Q) + n^3
-// (triangular product), and 2mn^2 for the final product -- against
+// Flops: QR of X 4mn^2 - 4n^3/3, per term 4n^3/3 (structured QR and Q) + 2n^3/3
+// (product of two triangular factors), and 2mn^2 for the final product -- against
 // r (4mn^2 + n^3) for r independent (m+n) x n stacks.
 // With `pf`, X = (the matrix pf factors) / scale: Q_x is pf's Q and R_x = R / scale, and
 // d_sqrtc must already hold scale * sqrt(c_j) ([R/scale; sqrt(c) I] and [R; scale sqrt(c) I]
@@ -115,14 +115,15 @@ void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx
   orgqr(c, mtot, n, mt, Ws, T, Qs, rk, -1, true);
   Mat S{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
   for (int b = 0; b < rk; ++b) {
-    // S += w_b Q1'_b Q2'_b^T; Q2'_b^T is lower triangular, so k starts at the output column
+    // S += w_b Q1'_b Q2'_b^T.  [R_x; sqrt(c) I] = Q'_b R_b gives Q1'_b = R_x R_b^{-1} and
+    // Q2'_b = sqrt(c) R_b^{-1}, both upper triangular: entry (i, j) needs k >= max(i, j)
     const Mat Qb{Qs.p + b * Qs.stride, lds, 0};
-    gemm(c, 0, 1, n, n, n, hw[b] / fone, Qb, Qb.at(mt, 0), b == 0 ? 0.0 : 1.0, S, 1, nullptr, 0, 1);
+    gemm(c, 0, 1, n, n, n, hw[b] / fone, Qb, Qb.at(mt, 0), b == 0 ? 0.0 : 1.0, S, 1, nullptr, 0, 3);
   }
   gemm(c, 0, 0, m, n, n, 1.0, Qx, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
   const double dm = m, dn = n;
   const double executed = (pf ? 2.0 : 4.0) * dm * dn * dn - (pf ? 2.0 : 4.0) * dn * dn * dn / 3.0 +
-                          rk * (7.0 * dn * dn * dn / 3.0) + 2.0 * dm * dn * dn;
+                          rk * (2.0 * dn * dn * dn) + 2.0 * dm * dn * dn;
   c.stats.flops_exec_delta += executed - rk * (4.0 * dm * dn * dn + dn * dn * dn);
 }
 
@@ -251,7 +252,8 @@ int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda
     *beta = 0.0;
     return 1;
   }
-  *beta = temp_beta / (std::sqrt(static_cast<double>(n)) * inv1);
+  // sigma_min(X) = 1/||R^{-1}||_2 >= 1/||R^{-1}||_F >= 1/(sqrt(n) ||R^{-1}||_1)
+  *beta = mode == BOUNDS_FROB ? 1.0 / std::sqrt(fr) : temp_beta / (std::sqrt(static_cast<double>(n)) * inv1);
   return 0;
 }
 
@@ -536,7 +538,7 @@ int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, 
   EventTimer total(c.stream());
   double alpha = 0.0, beta = 0.0;
   EventTimer tb(c.stream());
-  const int binfo = bounds(c, m, n, 0.0, dA, lda, BOUNDS_ZOLOPD, &alpha, &beta);
+  const int binfo = bounds(c, m, n, 0.0, dA, lda, c.zolo_beta_frob ? BOUNDS_FROB : BOUNDS_ZOLOPD, &alpha, &beta);
   const double ms_bounds = tb.stop();
   const double bflops = 4.0 / 3.0 * static_cast<double>(n) * n * n + 2.0 * m * static_cast<double>(n) * n;
   if (binfo != 0) {

@@ -10,6 +10,7 @@ namespace zolo {
 enum BoundsMode {
   BOUNDS_PQDWHFACS = 0,  // beta = ||X0||_1 / (sqrt(n) ||R^-1||_1)   (pqdwhfacs.f90:325-344 form)
   BOUNDS_ZOLOPD = 1,     // beta = 1 / (sqrt(n) ||R^-1||_1)           (zolopd.f90 / test_zolodrv1.f90 form)
+  BOUNDS_FROB = 2,       // beta = 1 / ||R^-1||_F: still <= sigma_min(X0), never below mode 1's
 };
 
 // alpha = ||A - sigma I||_F ; beta from R of (A - sigma I)/alpha = QR.  Returns info (0 ok).

@@ -345,6 +345,21 @@ __global__ void extract_v_kernel(int m, int w, const double* __restrict__ A, int
   }
 }
 
+// TB (jb x jb) <- the block diagonal of consecutive panels' T factors (QW x QW each, ld QW,
+// QW*QW apart), zero elsewhere: the diagonal of the block reflector's T.
+__global__ void block_t_init_kernel(int jb, const double* __restrict__ T, int64_t strideT, double* TB,
+                                    int64_t ldtb, int64_t strideTB) {
+  const double* Tb = T + blockIdx.y * strideT;
+  double* Bb = TB + blockIdx.y * strideTB;
+  const int total = jb * jb;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int i = e % jb, j = e / jb;
+    const int q = i / QW;
+    const double v = (q == j / QW && i <= j) ? Tb[q * QW * QW + (i % QW) + (j % QW) * QW] : 0.0;
+    Bb[i + static_cast<int64_t>(j) * ldtb] = v;
+  }
+}
+
 // P(:,col) <- T^T P(:,col)  or  T P(:,col), T upper triangular w x w (ld QW)
 __global__ void apply_t_kernel(int w, int n, const double* __restrict__ T, int64_t strideT, double* P,
                                int64_t ldp, int64_t strideP, int trans) {
@@ -486,6 +501,14 @@ cudaError_t extract_v(int m, int w, const double* A, int64_t lda, int64_t stride
   if (!(split > 0 && gap > 0)) split = m;
   int blocks = static_cast<int>(std::min<int64_t>((static_cast<int64_t>(m) * w + 255) / 256, 2048));
   extract_v_kernel<<<dim3(blocks, batch), 256, 0, st>>>(m, w, A, lda, strideA, V, ldv, strideV, split, gap);
+  return cudaGetLastError();
+}
+
+cudaError_t block_t_init(int jb, const double* T, int64_t strideT, double* TB, int64_t ldtb, int64_t strideTB,
+                         int batch, cudaStream_t st) {
+  if (jb <= 0 || batch <= 0) return cudaSuccess;
+  const int blocks = (jb * jb + 255) / 256;
+  block_t_init_kernel<<<dim3(blocks, batch), 256, 0, st>>>(jb, T, strideT, TB, ldtb, strideTB);
   return cudaGetLastError();
 }
 
