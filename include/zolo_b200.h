@@ -64,6 +64,9 @@ typedef struct {
                             does fewer than the canonical count)           */
   int ns_steps;        /* Newton-Schulz steps that ended the iteration     */
   int ns_finish;       /* 1 if Newton-Schulz steps ended the iteration     */
+  double ms_step[16];  /* per Zolo-PD / QDWH iteration: device milliseconds */
+  double ms_finish;    /* ZOLO_OPT_NS_FINISH: device ms from the check that
+                          entered the finish to its end (0 if not entered)   */
 } zolo_stats_t;
 
 /* ---- handles (no reference counterpart: the reference is one MPI job) ---- */

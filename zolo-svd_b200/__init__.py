@@ -50,6 +50,8 @@ class Stats(C.Structure):
         ("flops_executed", C.c_double),
         ("ns_steps", C.c_int),
         ("ns_finish", C.c_int),
+        ("ms_step", C.c_double * 16),
+        ("ms_finish", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -61,7 +63,8 @@ class Stats(C.Structure):
                     con=list(self.con[: min(it, 16)]), err=list(self.err[: min(it, 16)]),
                     branches=[{1: "QR", 2: "CH", 3: "NS"}.get(b, "?")
                               for b in self.branch[: min(it + self.ns_steps, 16)]],
-                    flops_executed=self.flops_executed, ns_steps=self.ns_steps, ns_finish=self.ns_finish)
+                    flops_executed=self.flops_executed, ns_steps=self.ns_steps, ns_finish=self.ns_finish,
+                    ms_step=list(self.ms_step[: min(it, 16)]), ms_finish=self.ms_finish)
 
 
 # (name, restype, argtypes)

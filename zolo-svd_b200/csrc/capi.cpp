@@ -281,6 +281,8 @@ int zolo_get_stats(zolo_handle_t h, zolo_stats_t* out) {
   out->flops_executed = s.flops + s.flops_exec_delta;
   out->ns_steps = s.ns_steps;
   out->ns_finish = s.ns_finish;
+  for (int i = 0; i < 16; ++i) out->ms_step[i] = s.ms_step[i];
+  out->ms_finish = s.ms_finish;
   return 0;
 }
 

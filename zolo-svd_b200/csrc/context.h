@@ -27,6 +27,8 @@ struct Stats {
   double flops_exec_delta = 0.0;  // executed minus canonical flops (shared-QR form: < 0)
   int ns_steps = 0;
   int ns_finish = 0;  // 1 if Newton-Schulz steps ended the iteration
+  double ms_step[16] = {0};  // device ms of each iteration
+  double ms_finish = 0.0;    // device ms of the Newton-Schulz finish (check included)
 };
 
 // Optional per-kernel-class timing with CUDA events recorded around launches on

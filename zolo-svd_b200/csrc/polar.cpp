@@ -228,7 +228,8 @@ int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda
     c.stats.launches += 2;
     temp_beta = d2h(c, scal + 1);
   }
-  // R of X = QR (unstructured Householder), then ||R^{-1}||_1 from R^{-1} = I * (R^T)^{-T}
+  // R of X = QR (unstructured Householder), then R^{-T} = (R^T)^{-1} by the blocked triangular
+  // inverse and R^{-1} as its transpose for ||R^{-1}||_1 and ||R^{-1}||_F
   double* tau = c.buf("bnd_tau", n);
   double* T = c.buf("bnd_t", static_cast<size_t>(npanels(n)) * 1024);
   geqrf(c, m, n, -1, Mat{X, ldx, 0}, tau, T, 1);
@@ -236,11 +237,12 @@ int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda
   double* I = c.buf("bnd_i", static_cast<size_t>(ldn) * n);
   double* Ri = c.buf("bnd_rinv", static_cast<size_t>(ldn) * n);
   ck(transpose(n, n, X, ldx, Lt, ldn, c.stream()));
-  ck(set_identity(n, n, I, ldn, 0, 1, 1.0, c.stream()));
-  c.stats.launches += 2;
+  c.stats.launches++;
   DiagInv D{c.buf("bnd_dinv", static_cast<size_t>(nblocks(n)) * 4096), 0};
   diag_inverses(c, n, Mat{Lt, ldn, 0}, 1, D);
-  trsm_rlt(c, n, n, Mat{Lt, ldn, 0}, Mat{I, ldn, 0}, Mat{Ri, ldn, 0}, 1, D);
+  trtri_lower(c, n, Mat{Lt, ldn, 0}, Mat{I, ldn, 0}, 1, D);
+  ck(transpose(n, n, I, ldn, Ri, ldn, c.stream()));
+  c.stats.launches++;
   double* colsum = c.buf("bnd_colsum", n);
   ck(norm1(n, n, Ri, ldn, colsum, scal + 2, c.stream()));
   ck(frob2(n, n, Ri, ldn, part, scal + 3, c.stream()));
@@ -306,6 +308,7 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
   double lowk = beta, err = 1.0, err2 = std::fabs(1.0 - lowk);
   int it = 0;
   while ((it == 0 || err > tol2 || err2 > tol1) && (o.maxit < 0 || it <= o.maxit) && it < 100) {
+    EventTimer tstep(c.stream());
     double ak, bk, ckk, lnext;
     qdwh_weights(lowk, &ak, &bk, &ckk, &lnext);
     lowk = lnext;
@@ -351,6 +354,7 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
     if (it < 16) {
       c.stats.con[it] = ckk;
       c.stats.err[it] = err;
+      c.stats.ms_step[it] = tstep.stop();
     }
     ++it;
     err2 = std::fabs(1.0 - lowk);
@@ -412,6 +416,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   const bool ns_finish = c.zolo_ns_finish != 0;
   EventTimer ti(c.stream());
   while (err > tol2 && it < maxit) {
+    EventTimer tstep(c.stream());
     compute_coeff(con, tol, rk, coeff.data());
     double maxc = coeff[0];
     for (int i = 1; i < 2 * rk; ++i) maxc = std::max(maxc, coeff[i]);
@@ -428,6 +433,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         if (e0 <= kNsEnter) {
           newton_schulz_finish(c, m, n, X, ldx, G, Z, e0, it);
           c.stats.ns_finish = 1;
+          c.stats.ms_finish = tstep.stop();
           break;
         }
       }
@@ -509,6 +515,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     if (it < 16) {
       c.stats.con[it] = con;
       c.stats.err[it] = err;
+      c.stats.ms_step[it] = tstep.stop();
     }
     con = con_next;
     ++it;
