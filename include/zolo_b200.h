@@ -67,6 +67,9 @@ typedef struct {
   double ms_step[16];  /* per Zolo-PD / QDWH iteration: device milliseconds */
   double ms_finish;    /* ZOLO_OPT_NS_FINISH: device ms from the check that
                           entered the finish to its end (0 if not entered)   */
+  int terms[16];       /* per Zolo-PD iteration: Zolotarev terms used (rk,
+                          or fewer in the iteration a Newton-Schulz finish
+                          follows, see ZOLO_OPT_NS_FINISH)                   */
 } zolo_stats_t;
 
 /* ---- handles (no reference counterpart: the reference is one MPI job) ---- */
@@ -103,7 +106,12 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * iterations, re-measuring e before each step and stopping at rounding level
  * (max(1e-14, eps sqrt(m)/2), or when a step no longer halves e; at most 12 steps,
  * none when e is already there).  The polar factor of X is that of A, so the result
- * agrees with the reference rule's to rounding.  No reference counterpart. */
+ * agrees with the reference rule's to rounding.  With ZOLO_OPT_CHOL_INVERSE as well, a
+ * Cholesky-form iteration takes the r <= rk Zolotarev terms that minimise its cost plus
+ * that of the Newton-Schulz steps it leaves (r n^3 + k(r) 3mn^2, k(r) from CON_next(r)),
+ * when the initial CON = 1/beta is at most 1e15 (beyond that the Zolotarev coefficients,
+ * alpha = acos(1/CON), are too inexact for CON_next to predict the iterate);
+ * zolo_stats_t.terms records r.  No reference counterpart. */
 #define ZOLO_OPT_NS_FINISH 2
 /* ZOLO_OPT_CHOL_INVERSE: 0 (default) = each Cholesky-form term solves
  * X (X^T X + c_j I)^{-1} with two triangular solves (zolochol.f90:87-113); 1 = the

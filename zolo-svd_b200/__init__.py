@@ -52,6 +52,7 @@ class Stats(C.Structure):
         ("ns_finish", C.c_int),
         ("ms_step", C.c_double * 16),
         ("ms_finish", C.c_double),
+        ("terms", C.c_int * 16),
     ]
 
     def as_dict(self) -> dict:
@@ -64,7 +65,8 @@ class Stats(C.Structure):
                     branches=[{1: "QR", 2: "CH", 3: "NS"}.get(b, "?")
                               for b in self.branch[: min(it + self.ns_steps, 16)]],
                     flops_executed=self.flops_executed, ns_steps=self.ns_steps, ns_finish=self.ns_finish,
-                    ms_step=list(self.ms_step[: min(it, 16)]), ms_finish=self.ms_finish)
+                    ms_step=list(self.ms_step[: min(it, 16)]), ms_finish=self.ms_finish,
+                    terms=list(self.terms[: min(it, 16)]))
 
 
 # (name, restype, argtypes)

@@ -283,6 +283,7 @@ int zolo_get_stats(zolo_handle_t h, zolo_stats_t* out) {
   out->ns_finish = s.ns_finish;
   for (int i = 0; i < 16; ++i) out->ms_step[i] = s.ms_step[i];
   out->ms_finish = s.ms_finish;
+  for (int i = 0; i < 16; ++i) out->terms[i] = s.terms[i];
   return 0;
 }
 

@@ -29,6 +29,7 @@ struct Stats {
   int ns_finish = 0;  // 1 if Newton-Schulz steps ended the iteration
   double ms_step[16] = {0};  // device ms of each iteration
   double ms_finish = 0.0;    // device ms of the Newton-Schulz finish (check included)
+  int terms[16] = {0};       // Zolotarev terms of each iteration
 };
 
 // Optional per-kernel-class timing with CUDA events recorded around launches on

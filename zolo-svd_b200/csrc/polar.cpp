@@ -67,6 +67,43 @@ int npanels(int n) { return (n + 31) / 32; }
 // ||X^T X - I||_F / sqrt(n) and the cap on the number of steps
 constexpr double kNsEnter = 0.1;
 constexpr int kNsMaxSteps = 12;
+// The Zolotarev coefficients take alpha = acos(1/CON) (Auxil_Zolo.f90:171); alpha near pi/2
+// carries an absolute rounding error of ~1e-16, i.e. a relative error of ~1e-16 CON in the
+// modulus 1/CON.  Up to an initial CON of 1e15 the CON recursion still predicts the spread of
+// the iterate well enough to choose the term count of the last Cholesky iteration from it.
+constexpr double kConTrusted = 1e15;
+
+// Terms for a Cholesky-form Zolo-PD iteration that Newton-Schulz steps will finish
+// (ZOLO_OPT_NS_FINISH with ZOLO_OPT_CHOL_INVERSE): the r <= rk minimising
+//   r n^3 (Cholesky, triangular inverse and lower-triangle product of each term)
+//   + k(r) 3 m n^2 (Newton-Schulz steps: X p(G) and the next Gram),
+// where k(r) steps take e0 = 2 (CON_next(r) - 1) to the rounding floor with
+// e -> 0.75 e^2 (after the iteration the singular values lie in [1, CON_next]).
+// r = rk when no r <= rk brings e0 within the Newton-Schulz entry threshold.
+int finish_terms(double con, double tol, int rk, int m, int n) {
+  const double floor_e = std::max(1e-14, 0.5 * eps_precision() * std::sqrt(static_cast<double>(m)));
+  const double dm = m, dn = n;
+  std::vector<double> cf(3 * rk);
+  int best = rk;
+  double best_cost = -1.0;
+  for (int r = 1; r <= rk; ++r) {
+    compute_coeff(con, tol, r, cf.data());
+    const double fone = zolo_fone(cf.data(), r);
+    double e = 2.0 * (zolo_next_con(con, cf.data(), r, fone) - 1.0);
+    if (!(e <= 0.5 * kNsEnter)) continue;
+    int k = 0;
+    while (e > floor_e && k < kNsMaxSteps) {
+      e = 0.75 * e * e;
+      ++k;
+    }
+    const double cost = r * dn * dn * dn + k * 3.0 * dm * dn * dn;
+    if (best_cost < 0.0 || cost < best_cost) {
+      best_cost = cost;
+      best = r;
+    }
+  }
+  return best;
+}
 
 // Q1 * Q2^T of the explicit Q of the stacked matrix (Q2 starts at row mp, upper triangular).
 void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
@@ -422,6 +459,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     for (int i = 1; i < 2 * rk; ++i) maxc = std::max(maxc, coeff[i]);
     bool use_qr = (it == 0 || con > 1.0e3) && maxc > 3.0e2;
     bool z_summed = false;  // Z holds sum_j w_j Z_j / FONE already (one Z instead of r)
+    int rk_it = rk;         // terms of this iteration
     if (!use_qr) {
       gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       if (ns_finish) {
@@ -437,24 +475,37 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
           break;
         }
       }
-      for (int b = 0; b < rk; ++b) hv[b] = coeff[2 * b];
-      h2d(c, dvec, hv.data(), rk);
-      ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk, c.stream()));
-      ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * rk, c.stream()));
+      const bool inverse_form = c.zolo_chol_inverse && !left;
+      if (ns_finish && inverse_form && 1.0 / beta <= kConTrusted) {
+        // the iteration Newton-Schulz steps finish: fewer terms can be cheaper
+        const int rr = finish_terms(con, tol, rk, m, n);
+        if (rr != rk) {
+          rk_it = rr;
+          compute_coeff(con, tol, rk_it, coeff.data());
+        }
+      }
+      for (int b = 0; b < rk_it; ++b) hv[b] = coeff[2 * b];
+      h2d(c, dvec, hv.data(), rk_it);
+      ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk_it, c.stream()));
+      ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * rk_it, c.stream()));
       c.stats.launches += 2;
-      potrf(c, n, Wc, rk, dinfo, Dz);
-      const int pinfo = read_info(c, dinfo, rk);
+      potrf(c, n, Wc, rk_it, dinfo, Dz);
+      const int pinfo = read_info(c, dinfo, rk_it);
       if (pinfo != 0) {
         if (c.stats.info == 0) c.stats.info = pinfo;
         use_qr = true;  // fall back to the QR form for this step
-      } else if (c.zolo_chol_inverse && !left) {
+        if (rk_it != rk) {
+          rk_it = rk;
+          compute_coeff(con, tol, rk, coeff.data());
+        }
+      } else if (inverse_form) {
         // explicit form: S = sum_b w_b W_b^{-1}, W_b^{-1} = L_b^{-T} L_b^{-1}, then one Z = X S
-        const double fone_c = zolo_fone(coeff.data(), rk);
-        Mat Y{c.buf("zc_y", static_cast<size_t>(ldn) * n * rk), ldn, ldn * n};
-        trtri_lower(c, n, Wc, Y, rk, Dz);
+        const double fone_c = zolo_fone(coeff.data(), rk_it);
+        Mat Y{c.buf("zc_y", static_cast<size_t>(ldn) * n * rk_it), ldn, ldn * n};
+        trtri_lower(c, n, Wc, Y, rk_it, Dz);
         Mat S{c.buf("zc_s", static_cast<size_t>(ldn) * n), ldn, 0};
-        for (int b = 0; b < rk; ++b) {
-          const double w = -coeff[2 * rk + b] / fone_c;
+        for (int b = 0; b < rk_it; ++b) {
+          const double w = -coeff[2 * rk_it + b] / fone_c;
           gemm(c, 1, 0, n, n, n, w, Mat{Y.p + b * Y.stride, ldn, 0}, Mat{Y.p + b * Y.stride, ldn, 0},
                b == 0 ? 0.0 : 1.0, S, 1, nullptr, 1, 2);
         }
@@ -465,8 +516,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         c.stats.chol_iterations++;
         if (it < 16) c.stats.branch[it] = 2;
         const double dm = m, dn = n;
-        c.stats.flops += dm * dn * dn + rk * (dn * dn * dn / 3.0 + 2.0 * dm * dn * dn);
-        c.stats.flops_exec_delta += rk * (dn * dn * dn - 2.0 * dm * dn * dn) + 2.0 * dm * dn * dn;
+        c.stats.flops += dm * dn * dn + rk_it * (dn * dn * dn / 3.0 + 2.0 * dm * dn * dn);
+        c.stats.flops_exec_delta += rk_it * (dn * dn * dn - 2.0 * dm * dn * dn) + 2.0 * dm * dn * dn;
       } else {
         spd_solve(c, m, n, X, ldx, Wc, Dz, Z, rk, left);
         for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b];
@@ -476,8 +527,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
                          rk * (static_cast<double>(n) * n * n / 3.0 + 2.0 * m * static_cast<double>(n) * n);
       }
     }
-    const double fone = zolo_fone(coeff.data(), rk);
-    const double con_next = zolo_next_con(con, coeff.data(), rk, fone);
+    const double fone = zolo_fone(coeff.data(), rk_it);
+    const double con_next = zolo_next_con(con, coeff.data(), rk_it, fone);
     if (use_qr) {
       const bool shared = c.zolo_shared_qr != 0;
       z_summed = shared;
@@ -516,6 +567,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       c.stats.con[it] = con;
       c.stats.err[it] = err;
       c.stats.ms_step[it] = tstep.stop();
+      c.stats.terms[it] = rk_it;
     }
     con = con_next;
     ++it;
