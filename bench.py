@@ -216,13 +216,15 @@ def run_reference(args):
 # through S = sum_j w_j (X^T X + c_j I)^{-1} (explicit triangular inverses) and one
 # Z = X S, beta = 1/||R^{-1}||_F (a lower bound on sigma_min up to sqrt(n) tighter than
 # the reference driver's, which keeps CON = 1/beta where the Zolotarev coefficients are
-# accurate), and FP64 Newton-Schulz steps once ||X^T X - I||_F/sqrt(n) <= 0.1.
+# accurate), FP64 Newton-Schulz steps once ||X^T X - I||_F/sqrt(n) <= 0.1, and per
+# iteration the Zolotarev term count (<= r) of the cheapest plan to convergence on one GPU.
 # "reference_steps" runs the reference's own steps on the GPU as two calls (bounds, then PZOLOPD1): one
 # structured QR of [X; sqrt(c_j) I] per term and the reference's stopping rule
 # (pzolopd1.f90:381-397).
 FORMS = {
-    "fast": {"shared_qr": 1, "ns_finish": 1, "chol_inverse": 1, "beta_frob": 1, "one_call": True},
-    "reference_steps": {"shared_qr": 0, "ns_finish": 0, "chol_inverse": 0, "beta_frob": 0, "one_call": False},
+    "fast": {"shared_qr": 1, "ns_finish": 1, "chol_inverse": 1, "beta_frob": 1, "term_plan": 1, "one_call": True},
+    "reference_steps": {"shared_qr": 0, "ns_finish": 0, "chol_inverse": 0, "beta_frob": 0, "term_plan": 0,
+                        "one_call": False},
 }
 
 # DRAM bytes (read + write) of one launch of the dominant kernel (DMMA GEMM, 128x128 tiles)
@@ -277,6 +279,7 @@ def run_gpu(args):
         h.set_option(zb.OPT_NS_FINISH, FORMS[name]["ns_finish"])
         h.set_option(zb.OPT_CHOL_INVERSE, FORMS[name]["chol_inverse"])
         h.set_option(zb.OPT_BETA_FROB, FORMS[name]["beta_frob"])
+        h.set_option(zb.OPT_TERM_PLAN, FORMS[name]["term_plan"])
 
     def step(src):
         if FORMS[form["name"]]["one_call"]:
@@ -386,12 +389,12 @@ def run_gpu(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"Zolo-PD r={rk} (bounds + PZOLOPD1 + H), n={n}, kappa={args.kappa:g}, "
                                    f"FP64 on DMMA, fast form (one call, shared QR of X, explicit-inverse Cholesky "
-                                   f"iterations, Frobenius beta bound, Newton-Schulz finish)",
+                                   f"iterations, Frobenius beta bound, Newton-Schulz finish, planned term counts)",
                        "n": n, "rk": rk, "kappa": args.kappa, "form": "fast", "precision": "fp64",
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs 512 MiB per matrix > 126 MB L2 (no flush needed)"},
             "accuracy": dict(acc_fast, iterations=st_fast["iterations"], ns_steps=st_fast["ns_steps"],
-                             branches=st_fast["branches"]),
+                             branches=st_fast["branches"], terms=st_fast["terms"]),
             "forms": {
                 "fast": {"s": t_ms / 1e3, "backward_error": acc_fast["backward_error"],
                          "orthogonality": acc_fast["orthogonality"], "branches": st_fast["branches"]},

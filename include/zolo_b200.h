@@ -68,8 +68,7 @@ typedef struct {
   double ms_finish;    /* ZOLO_OPT_NS_FINISH: device ms from the check that
                           entered the finish to its end (0 if not entered)   */
   int terms[16];       /* per Zolo-PD iteration: Zolotarev terms used (rk,
-                          or fewer in the iteration a Newton-Schulz finish
-                          follows, see ZOLO_OPT_NS_FINISH)                   */
+                          or the planned count, see ZOLO_OPT_TERM_PLAN)      */
 } zolo_stats_t;
 
 /* ---- handles (no reference counterpart: the reference is one MPI job) ---- */
@@ -106,12 +105,8 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * iterations, re-measuring e before each step and stopping at rounding level
  * (max(1e-14, eps sqrt(m)/2), or when a step no longer halves e; at most 12 steps,
  * none when e is already there).  The polar factor of X is that of A, so the result
- * agrees with the reference rule's to rounding.  With ZOLO_OPT_CHOL_INVERSE as well, a
- * Cholesky-form iteration takes the r <= rk Zolotarev terms that minimise its cost plus
- * that of the Newton-Schulz steps it leaves (r n^3 + k(r) 3mn^2, k(r) from CON_next(r)),
- * when the initial CON = 1/beta is at most 1e15 (beyond that the Zolotarev coefficients,
- * alpha = acos(1/CON), are too inexact for CON_next to predict the iterate);
- * zolo_stats_t.terms records r.  No reference counterpart. */
+ * agrees with the reference rule's to rounding.  With this option the loop ends at that
+ * measured check rather than on ||X_{k+1} - X_k||.  No reference counterpart. */
 #define ZOLO_OPT_NS_FINISH 2
 /* ZOLO_OPT_CHOL_INVERSE: 0 (default) = each Cholesky-form term solves
  * X (X^T X + c_j I)^{-1} with two triangular solves (zolochol.f90:87-113); 1 = the
@@ -129,11 +124,29 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * one more is needed; the tighter beta keeps CON below that for condition numbers up to
  * about 1e13.  No reference counterpart. */
 #define ZOLO_OPT_BETA_FROB 4
+/* ZOLO_OPT_TERM_PLAN: 0 (default) = every Zolo-PD iteration takes rk terms; 1 = each
+ * iteration takes the r <= rk terms of the cheapest plan to convergence on one GPU.  The
+ * reference runs the r terms on r process groups at once; here they run one after another,
+ * so an iteration costs a fixed part plus r times a term and fewer terms per iteration can
+ * converge sooner.  Before each iteration the CON recursion (pzolopd1.f90:459-472) is
+ * searched over the next three iterations and the Newton-Schulz finish with a cost model of
+ * this implementation, and the finish is entered from the measured e only when cheaper than
+ * the plan; an iteration takes the QR form while CON > 12 (the Cholesky form's error grows
+ * with CON).  The coefficients are those of zolo_compute_coeff_kp (exact at any CON, so the
+ * recursion predicts the iterate).  Applies with ZOLO_OPT_NS_FINISH and
+ * ZOLO_OPT_CHOL_INVERSE (SYM = 'N'); otherwise rk terms.  zolo_stats_t.terms records the
+ * counts.  No reference counterpart. */
+#define ZOLO_OPT_TERM_PLAN 5
 int zolo_set_option(zolo_handle_t handle, int option, int value);
 
 /* ---- host scalar routines (no GPU needed) ---- */
 /* Compute_Coeff (Auxil_Zolo.f90:165-200): coeff[0:2rk] = c_i, coeff[2rk:3rk] = -a_i. */
 int zolo_compute_coeff(double con, double tol, int rk, double* coeff);
+/* The same coefficients computed from the complementary modulus 1/CON directly (the AGM
+ * started from (1, 1/CON), and for 1/CON <= 1e-6 the near-unit-modulus expansions of sn, cn),
+ * accurate to ~1e-10 relative at any CON > 1, where Compute_Coeff's alpha = acos(1/CON) has a
+ * relative error of ~1e-16 CON.  Used by ZOLO_OPT_TERM_PLAN.  No reference counterpart. */
+int zolo_compute_coeff_kp(double con, double tol, int rk, double* coeff);
 /* mellipke (Auxil_Zolo.f90:36-71) */
 void zolo_mellipke(double alpha, double tol, double* k, double* e);
 /* MELLIPJ (Auxil_Zolo.f90:73-128) */

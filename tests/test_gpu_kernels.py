@@ -262,7 +262,8 @@ def _qr_gpu(h, w, m_top):
     return host(dw), dtau.cpu().numpy(), host(dq)
 
 
-@pytest.mark.parametrize("mn", [(1, 1), (5, 3), (40, 32), (100, 33), (300, 200), (1000, 96)])
+@pytest.mark.parametrize("mn", [(1, 1), (5, 3), (40, 32), (100, 33), (300, 200), (1000, 96), (700, 300), (513, 513),
+                                (1031, 260)])
 def test_geqrf_orgqr_unstructured_vs_lapack(h, mn):
     m, n = mn
     rng = np.random.default_rng(m * 7 + n)
@@ -276,7 +277,7 @@ def test_geqrf_orgqr_unstructured_vs_lapack(h, mn):
     assert np.allclose(q, q_ref, rtol=0, atol=tol)
 
 
-@pytest.mark.parametrize("mn", [(64, 64), (100, 70), (257, 129)])
+@pytest.mark.parametrize("mn", [(64, 64), (100, 70), (257, 129), (600, 300), (301, 257), (390, 390)])
 def test_structured_stack_qr(h, mn):
     """[X; sqrt(c) I]: the row-windowed factorisation gives LAPACK's Q and an exactly upper triangular Q2."""
     m, n = mn

@@ -396,12 +396,14 @@ def test_polar_dev_frobenius_beta(m, n, kappa):
     assert np.linalg.norm(q1 - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
 
 
-@pytest.mark.parametrize("m,n,kappa", [(300, 300, 1e12), (420, 250, 1e8), (129, 129, 1e16), (500, 500, 1e3)])
-def test_fast_form_all_options(m, n, kappa):
+@pytest.mark.parametrize("m,n,kappa", [(300, 300, 1e12), (420, 250, 1e8), (129, 129, 1e16), (500, 500, 1e3),
+                                        (256, 256, 1e14), (200, 200, 1.0)])
+@pytest.mark.parametrize("plan", [0, 1])
+def test_fast_form_all_options(m, n, kappa, plan):
     """All cost options together (shared QR, explicit-inverse Cholesky, Frobenius beta, Newton-Schulz
-    finish with the term count of the last Cholesky iteration chosen by cost): backward stable
-    (10 n eps), the same polar factor as the reference steps (Q within kappa eps), at most rk terms
-    in every iteration, fewer only in the Cholesky iteration the finish follows."""
+    finish, and with `plan` the per-iteration term counts of the cost plan): backward stable
+    (10 n eps, and below 1e-13), the same polar factor as the reference steps (Q within kappa eps),
+    1..rk terms in every iteration (rk in every iteration without the plan)."""
     import torch
     s = np.geomspace(1.0, 1.0 / kappa, n)
     a, u, v = zo.make_matrix(n, s, 660 + m + n, m=m)
@@ -411,16 +413,16 @@ def test_fast_form_all_options(m, n, kappa):
     dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
     for opt in (zb.OPT_SHARED_QR, zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_BETA_FROB):
         h.set_option(opt, 1)
+    h.set_option(zb.OPT_TERM_PLAN, plan)
     torch.cuda.synchronize()
     assert zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n) == 0
     st = h.stats()
     h.close()
     q, hh = zb.device_to_colmajor(dq), zb.device_to_colmajor(dh)
     check_pd(a, q, hh, n)
+    assert zo.backward_error(a, q, hh) <= 1e-13
     assert np.linalg.norm(q - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
     its = st["iterations"]
     assert len(st["terms"]) == its and all(1 <= t <= 8 for t in st["terms"])
-    for k in range(its - 1):
-        assert st["terms"][k] == 8  # only the last Zolo iteration may take fewer terms
-    if st["terms"][-1] < 8:
-        assert st["branches"][its - 1] == "CH" and st["ns_finish"] == 1
+    if not plan:
+        assert all(t == 8 for t in st["terms"])

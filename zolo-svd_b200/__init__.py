@@ -83,6 +83,7 @@ _SIGS = [
     ("zolo_profile_read", C.c_int, [C.c_void_p, c_double_p, C.c_int]),
     ("zolo_set_option", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
+    ("zolo_compute_coeff_kp", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_mellipke", None, [C.c_double, C.c_double, c_double_p, c_double_p]),
     ("zolo_mellipj", None, [C.c_double, C.c_double, C.c_double, c_double_p, c_double_p, c_double_p]),
     ("zolo_choosem", C.c_int, [C.c_double]),
@@ -142,6 +143,7 @@ OPT_SHARED_QR = 1
 OPT_NS_FINISH = 2
 OPT_CHOL_INVERSE = 3
 OPT_BETA_FROB = 4
+OPT_TERM_PLAN = 5
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
@@ -191,6 +193,15 @@ def compute_coeff(con: float, tol: float, rk: int) -> np.ndarray:
     r = lib().zolo_compute_coeff(con, tol, rk, _dp(out))
     if r != 0:
         raise ZoloError("zolo_compute_coeff", r)
+    return out
+
+
+def compute_coeff_kp(con: float, tol: float, rk: int) -> np.ndarray:
+    """Zolotarev coefficients from the complementary modulus 1/con (accurate at any con)."""
+    out = np.zeros(3 * rk)
+    r = lib().zolo_compute_coeff_kp(con, tol, rk, _dp(out))
+    if r != 0:
+        raise ZoloError("zolo_compute_coeff_kp", r)
     return out
 
 

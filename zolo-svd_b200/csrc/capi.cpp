@@ -239,6 +239,10 @@ int zolo_set_option(zolo_handle_t h, int option, int value) {
       c.zolo_beta_frob = value != 0;
       return 0;
     }
+    if (option == ZOLO_OPT_TERM_PLAN) {
+      c.zolo_term_plan = value != 0;
+      return 0;
+    }
     return -1;
   });
 }
@@ -291,6 +295,13 @@ int zolo_compute_coeff(double con, double tol, int rk, double* coeff) {
   if (rk < 1 || rk > 8 || !coeff) return -3;
   if (!(con >= 1.0)) return -1;
   zolo::compute_coeff(con, tol, rk, coeff);
+  return 0;
+}
+
+int zolo_compute_coeff_kp(double con, double tol, int rk, double* coeff) {
+  if (rk < 1 || rk > 8 || !coeff) return -3;
+  if (!(con > 1.0) || !std::isfinite(con)) return -1;
+  zolo::compute_coeff_kp(con, tol, rk, coeff);
   return 0;
 }
 void zolo_mellipke(double alpha, double tol, double* k, double* e) { zolo::mellipke(alpha, tol, k, e); }

@@ -97,6 +97,8 @@ class Context {
   int zolo_chol_inverse = 0;
   // zolo_polar's bounds: 0 = beta = 1/(sqrt(n) ||R^-1||_1) (test_zolodrv1.f90), 1 = 1/||R^-1||_F.
   int zolo_beta_frob = 0;
+  // Zolo-PD term counts: 0 = rk in every iteration, 1 = planned per iteration (r <= rk) by cost.
+  int zolo_term_plan = 0;
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles

@@ -67,43 +67,79 @@ int npanels(int n) { return (n + 31) / 32; }
 // ||X^T X - I||_F / sqrt(n) and the cap on the number of steps
 constexpr double kNsEnter = 0.1;
 constexpr int kNsMaxSteps = 12;
-// The Zolotarev coefficients take alpha = acos(1/CON) (Auxil_Zolo.f90:171); alpha near pi/2
-// carries an absolute rounding error of ~1e-16, i.e. a relative error of ~1e-16 CON in the
-// modulus 1/CON.  Up to an initial CON of 1e15 the CON recursion still predicts the spread of
-// the iterate well enough to choose the term count of the last Cholesky iteration from it.
-constexpr double kConTrusted = 1e15;
 
-// Terms for a Cholesky-form Zolo-PD iteration that Newton-Schulz steps will finish
-// (ZOLO_OPT_NS_FINISH with ZOLO_OPT_CHOL_INVERSE): the r <= rk minimising
-//   r n^3 (Cholesky, triangular inverse and lower-triangle product of each term)
-//   + k(r) 3 m n^2 (Newton-Schulz steps: X p(G) and the next Gram),
-// where k(r) steps take e0 = 2 (CON_next(r) - 1) to the rounding floor with
-// e -> 0.75 e^2 (after the iteration the singular values lie in [1, CON_next]).
-// r = rk when no r <= rk brings e0 within the Newton-Schulz entry threshold.
-int finish_terms(double con, double tol, int rk, int m, int n) {
-  const double floor_e = std::max(1e-14, 0.5 * eps_precision() * std::sqrt(static_cast<double>(m)));
-  const double dm = m, dn = n;
-  std::vector<double> cf(3 * rk);
-  int best = rk;
-  double best_cost = -1.0;
-  for (int r = 1; r <= rk; ++r) {
-    compute_coeff(con, tol, r, cf.data());
-    const double fone = zolo_fone(cf.data(), r);
-    double e = 2.0 * (zolo_next_con(con, cf.data(), r, fone) - 1.0);
-    if (!(e <= 0.5 * kNsEnter)) continue;
+// Term plan of Zolo-PD on one GPU (ZOLO_OPT_TERM_PLAN).  The reference runs the r terms
+// of an iteration on r process groups at once, so r costs it no time; on one GPU the terms
+// run one after another and an iteration costs a fixed part plus r times a term.  Before
+// each iteration the planner searches the term counts of the next iterations (up to three,
+// then the Newton-Schulz finish) through the CON recursion and takes the first count of the
+// cheapest sequence.  An iteration takes the QR form while CON > kConChol: the Cholesky form
+// at CON solves with matrices of condition up to CON^2 and its error grows with it (measured
+// backward errors 7e-15, 3e-14 and 5e-13 for a first Cholesky iteration at CON 2, 32 and 224).
+// The coefficients come from compute_coeff_kp, exact at any CON, so the recursion predicts
+// the iterate.  Costs in units of n^3 flops at the measured GEMM rate, from the kernel times
+// at n = 8192; the parts that scale with m are multiplied by m/n.
+constexpr double kConChol = 12.0;
+class TermPlanner {
+ public:
+  TermPlanner(int rk, int m, int n, double tol) : rk_(rk), mu_(static_cast<double>(m) / n), tol_(tol) {
+    floor_e_ = std::max(1e-14, 0.5 * eps_precision() * std::sqrt(static_cast<double>(m)));
+  }
+  // terms for the iteration at CON = con; `prefactored`: the QR of X is at hand (first iteration)
+  int choose(double con, bool prefactored) {
+    int first = rk_;
+    plan(con, prefactored, 3, &first);
+    return first;
+  }
+  // cost of the cheapest plan from CON at a Cholesky iteration whose Gram is already formed
+  double cost_from(double con) { return plan(con, false, 3, nullptr) - (con > kConChol ? 0.0 : mu_ * kNsEntry); }
+  // Newton-Schulz steps from a measured e to the rounding floor
+  double ns_cost(double e) const { return mu_ * kNsStep * ns_steps(e); }
+
+ private:
+  static constexpr double kQrTerm = 2.6, kQrFixedPre = 7.3, kQrOfX = 3.9;
+  static constexpr double kChTerm = 1.2, kChFixed = 2.9, kNsStep = 2.95, kNsEntry = 1.0;
+  int rk_;
+  double mu_, tol_, floor_e_;
+  std::map<std::pair<double, int>, double> next_;
+
+  double next_con(double con, int r) {
+    const auto key = std::make_pair(con, r);
+    const auto it = next_.find(key);
+    if (it != next_.end()) return it->second;
+    double cf[24];
+    compute_coeff_kp(con, tol_, r, cf);
+    const double v = zolo_next_con(con, cf, r, zolo_fone(cf, r));
+    next_[key] = v;
+    return v;
+  }
+  int ns_steps(double e) const {
     int k = 0;
-    while (e > floor_e && k < kNsMaxSteps) {
+    while (e > floor_e_ && k < kNsMaxSteps) {
       e = 0.75 * e * e;
       ++k;
     }
-    const double cost = r * dn * dn * dn + k * 3.0 * dm * dn * dn;
-    if (best_cost < 0.0 || cost < best_cost) {
-      best_cost = cost;
-      best = r;
-    }
+    return k;
   }
-  return best;
-}
+  double plan(double con, bool prefactored, int depth, int* first) {
+    const double e = 2.0 * (con - 1.0);
+    if (e <= 0.5 * kNsEnter) return mu_ * (kNsEntry + ns_steps(e) * kNsStep);
+    if (depth == 0) return 1e300;
+    const bool qr = con > kConChol;
+    const double fixed = qr ? mu_ * (kQrFixedPre + (prefactored ? 0.0 : kQrOfX)) : mu_ * kChFixed;
+    double best = 1e300;
+    for (int r = 1; r <= rk_; ++r) {
+      const double here = fixed + r * (qr ? kQrTerm : kChTerm);
+      if (here >= best) break;  // the cost of this iteration grows with r
+      const double tot = here + plan(next_con(con, r), false, depth - 1, nullptr);
+      if (tot < best) {
+        best = tot;
+        if (first) *first = r;
+      }
+    }
+    return best;
+  }
+};
 
 // Q1 * Q2^T of the explicit Q of the stacked matrix (Q2 starts at row mp, upper triangular).
 void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
@@ -452,14 +488,22 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   int it = 0;
   const bool ns_finish = c.zolo_ns_finish != 0;
   EventTimer ti(c.stream());
-  while (err > tol2 && it < maxit) {
+  // term plan (ZOLO_OPT_TERM_PLAN): needs the measured Newton-Schulz finish to end the loop;
+  // its coefficients come from the complementary modulus (exact at any CON)
+  const bool plan_terms = ns_finish && c.zolo_term_plan && c.zolo_chol_inverse && !left;
+  TermPlanner planner(rk, m, n, tol);
+  int planned = 0;
+  // with the Newton-Schulz finish the loop ends at the measured check, not on ||X_{k+1} - X_k||
+  while ((ns_finish || err > tol2) && it < maxit) {
     EventTimer tstep(c.stream());
-    compute_coeff(con, tol, rk, coeff.data());
+    int rk_it = rk;  // terms of this iteration
+    if (plan_terms) rk_it = planned > 0 ? planned : planner.choose(con, it == 0 && pf && c.zolo_shared_qr);
+    if (plan_terms) compute_coeff_kp(con, tol, rk_it, coeff.data());
+    else compute_coeff(con, tol, rk_it, coeff.data());
     double maxc = coeff[0];
-    for (int i = 1; i < 2 * rk; ++i) maxc = std::max(maxc, coeff[i]);
-    bool use_qr = (it == 0 || con > 1.0e3) && maxc > 3.0e2;
+    for (int i = 1; i < 2 * rk_it; ++i) maxc = std::max(maxc, coeff[i]);
+    bool use_qr = plan_terms ? con > kConChol : (it == 0 || con > 1.0e3) && maxc > 3.0e2;
     bool z_summed = false;  // Z holds sum_j w_j Z_j / FONE already (one Z instead of r)
-    int rk_it = rk;         // terms of this iteration
     if (!use_qr) {
       gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       if (ns_finish) {
@@ -468,7 +512,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         ck(ns_prepare(n, G.p, G.ld, part, scal + 2, 0, c.stream()));
         c.stats.launches += 2;
         const double e0 = std::sqrt(d2h(c, scal + 2) / n);
-        if (e0 <= kNsEnter) {
+        // with the term plan: Newton-Schulz from the measured e0 only when cheaper than the plan
+        if (e0 <= kNsEnter && (!plan_terms || planner.ns_cost(e0) <= planner.cost_from(con))) {
           newton_schulz_finish(c, m, n, X, ldx, G, Z, e0, it);
           c.stats.ns_finish = 1;
           c.stats.ms_finish = tstep.stop();
@@ -476,14 +521,6 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         }
       }
       const bool inverse_form = c.zolo_chol_inverse && !left;
-      if (ns_finish && inverse_form && 1.0 / beta <= kConTrusted) {
-        // the iteration Newton-Schulz steps finish: fewer terms can be cheaper
-        const int rr = finish_terms(con, tol, rk, m, n);
-        if (rr != rk) {
-          rk_it = rr;
-          compute_coeff(con, tol, rk_it, coeff.data());
-        }
-      }
       for (int b = 0; b < rk_it; ++b) hv[b] = coeff[2 * b];
       h2d(c, dvec, hv.data(), rk_it);
       ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk_it, c.stream()));
@@ -494,10 +531,6 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       if (pinfo != 0) {
         if (c.stats.info == 0) c.stats.info = pinfo;
         use_qr = true;  // fall back to the QR form for this step
-        if (rk_it != rk) {
-          rk_it = rk;
-          compute_coeff(con, tol, rk, coeff.data());
-        }
       } else if (inverse_form) {
         // explicit form: S = sum_b w_b W_b^{-1}, W_b^{-1} = L_b^{-T} L_b^{-1}, then one Z = X S
         const double fone_c = zolo_fone(coeff.data(), rk_it);
@@ -519,12 +552,12 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         c.stats.flops += dm * dn * dn + rk_it * (dn * dn * dn / 3.0 + 2.0 * dm * dn * dn);
         c.stats.flops_exec_delta += rk_it * (dn * dn * dn - 2.0 * dm * dn * dn) + 2.0 * dm * dn * dn;
       } else {
-        spd_solve(c, m, n, X, ldx, Wc, Dz, Z, rk, left);
-        for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b];
+        spd_solve(c, m, n, X, ldx, Wc, Dz, Z, rk_it, left);
+        for (int b = 0; b < rk_it; ++b) hv[16 + b] = -coeff[2 * rk_it + b];
         c.stats.chol_iterations++;
         if (it < 16) c.stats.branch[it] = 2;
         c.stats.flops += static_cast<double>(m) * n * n +
-                         rk * (static_cast<double>(n) * n * n / 3.0 + 2.0 * m * static_cast<double>(n) * n);
+                         rk_it * (static_cast<double>(n) * n * n / 3.0 + 2.0 * m * static_cast<double>(n) * n);
       }
     }
     const double fone = zolo_fone(coeff.data(), rk_it);
@@ -534,21 +567,21 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       z_summed = shared;
       // the first iteration may reuse the QR of A/alpha: X0 = (A/alpha)/beta
       const Prefactored* pfi = (shared && it == 0) ? pf : nullptr;
-      for (int b = 0; b < rk; ++b) hv[b] = std::sqrt(coeff[2 * b]) * (pfi ? beta : 1.0);
-      h2d(c, dvec, hv.data(), rk);
-      for (int b = 0; b < rk; ++b) hv[16 + b] = -coeff[2 * rk + b] / std::sqrt(coeff[2 * b]);
+      for (int b = 0; b < rk_it; ++b) hv[b] = std::sqrt(coeff[2 * b]) * (pfi ? beta : 1.0);
+      h2d(c, dvec, hv.data(), rk_it);
+      for (int b = 0; b < rk_it; ++b) hv[16 + b] = -coeff[2 * rk_it + b] / std::sqrt(coeff[2 * b]);
       if (shared) {
-        zolo_terms_shared_qr(c, m, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk, pfi);
+        zolo_terms_shared_qr(c, m, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk_it, pfi);
       } else {
-        ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk, c.stream()));
+        ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk_it, c.stream()));
         c.stats.launches++;
-        geqrf(c, mp + n, n, mp, W, tau, T, rk);
-        orgqr(c, mp + n, n, mp, W, T, Qf, rk);
-        q1q2t(c, m, mp, n, Qf, Z, rk);
+        geqrf(c, mp + n, n, mp, W, tau, T, rk_it);
+        orgqr(c, mp + n, n, mp, W, T, Qf, rk_it);
+        q1q2t(c, m, mp, n, Qf, Z, rk_it);
       }
       // canonical: the reference's structured QR form, 4mn^2 + n^3 per term (the shared form
       // records what it executes beyond this in flops_exec_delta)
-      c.stats.flops += rk * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
+      c.stats.flops += rk_it * (4.0 * m * static_cast<double>(n) * n + static_cast<double>(n) * n * n);
       c.stats.qr_iterations++;
       if (it < 16) c.stats.branch[it] = 1;
     }
@@ -556,12 +589,14 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       // Z already holds sum_j w_j Z_j / FONE
       ck(combine_update(m, n, X, ldx, Z.p, Z.ld, 0, 1, 1.0 / fone, 1.0, nullptr, part, scal, c.stream()));
     } else {
-      for (int b = 0; b < rk; ++b) hv[16 + b] /= fone;
-      h2d(c, dvec + 16, hv.data() + 16, rk);
-      ck(combine_update(m, n, X, ldx, Z.p, Z.ld, Z.stride, rk, 1.0 / fone, 0.0, dvec + 16, part, scal,
+      for (int b = 0; b < rk_it; ++b) hv[16 + b] /= fone;
+      h2d(c, dvec + 16, hv.data() + 16, rk_it);
+      ck(combine_update(m, n, X, ldx, Z.p, Z.ld, Z.stride, rk_it, 1.0 / fone, 0.0, dvec + 16, part, scal,
                         c.stream()));
     }
     c.stats.launches += 2;
+    // plan the next iteration while this one runs
+    if (plan_terms) planned = planner.choose(con_next, false);
     err = std::sqrt(d2h(c, scal));
     if (it < 16) {
       c.stats.con[it] = con;
