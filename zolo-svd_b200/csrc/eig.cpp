@@ -304,9 +304,8 @@ int svd(Context& c, int m, int n, const double* dA, int64_t lda, int algo, int r
     QdwhOpts o;
     info = qdwh(c, m, n, dA, lda, Q, ldm, H, ldn, o);
   } else {
-    double alpha, beta;
-    info = bounds(c, m, n, 0.0, dA, lda, BOUNDS_ZOLOPD, &alpha, &beta);
-    if (info == 0) info = zolo_pd(c, 'N', rk, m, n, alpha, beta, dA, lda, Q, ldm, H, ldn);
+    // bounds + Zolo-PD + H; the first QR iteration reuses the bounds' QR of A/alpha
+    info = zolo_polar(c, rk, m, n, dA, lda, Q, ldm, H, ldn);
   }
   if (info != 0) return info;
   const Stats pd = c.stats;

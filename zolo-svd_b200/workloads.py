@@ -6,12 +6,14 @@ matrices A = U diag(s) V^T with Haar U, V and the stated spectra:
 
   c1  QDWH-PD (PQDWHFACS), n = 1024, s geometric in [1e-8, 1]
   c2  Zolo-PD r = 8, n = 4096, s geometric in [1e-16, 1] with 5 % duplicated values,
-      reference stopping rule and Newton-Schulz finish
+      reference stopping rule, Newton-Schulz finish, and the fast form (zolo_polar_dev
+      with every cost option)
   c4  512 matrices, n log-uniform in [64, 1024], m = n (1 + U[0, 1]), kappa
       log-uniform in [1e2, 1e14], s geometric: batched QDWH-PD (zolo_qdwh_batch_dev)
       against one zolo_qdwh_dev call per matrix
   c5  Zolo-SVD (Zolo-PD r = 8 + eigensolver of H), 16384 x 8192: 70 % of s geometric
-      in [1e-10, 1], 20 % exactly 1, 10 % in clusters of relative gap 1e-9
+      in [1e-10, 1], 20 % exactly 1, 10 % in clusters of relative gap 1e-9; with the
+      fast options, with the reference's steps, and with QDWH as the polar step
 
 Device times are CUDA events around the calls on the handle's stream (inputs
 resident in HBM, a warm-up call first).
@@ -63,6 +65,11 @@ def main(argv) -> int:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    def set_fast(on):
+        # the cost options of the fast form (each changes the cost, not the result beyond rounding)
+        for opt in (zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_BETA_FROB, zb.OPT_TERM_PLAN):
+            h.set_option(opt, 1 if on else 0)
+
     def pd_errors(a, q, hh, s=None):
         n = q.shape[1]
         out = {"backward_error": float(torch.linalg.norm(a - q @ hh) / torch.linalg.norm(a)),
@@ -101,19 +108,23 @@ def main(argv) -> int:
             a = (u * s[None, :]) @ v.T
             da = a.T.contiguous()
             dq, dh = torch.empty_like(da), torch.empty_like(da)
-            for nsf in (0, 1):
-                h.set_option(zb.OPT_NS_FINISH, nsf)
+            for form in ("reference_rule", "ns_finish", "fast"):
+                set_fast(form == "fast")
+                h.set_option(zb.OPT_NS_FINISH, 0 if form == "reference_rule" else 1)
 
                 def run():
+                    if form == "fast":
+                        zb.polar_dev(h, 8, n, n, da.data_ptr(), n, dq.data_ptr(), n, dh.data_ptr(), n)
+                        return
                     al, be, _ = zb.bounds_dev(h, n, n, da.data_ptr(), n, mode=1)
                     zb.pzolopd1_dev(h, "N", 8, n, n, al, be, da.data_ptr(), n, dq.data_ptr(), n, dh.data_ptr(), n)
                 ms = timed(run, reps=3)
                 stt = h.stats()
-                line = {"workload": "c2 Zolo-PD r=8 n=4096 kappa=1e16 clustered",
-                        "form": "ns_finish" if nsf else "reference_rule", "ms": ms, "branches": stt["branches"]}
+                line = {"workload": "c2 Zolo-PD r=8 n=4096 kappa=1e16 clustered", "form": form, "ms": ms,
+                        "branches": stt["branches"], "terms": stt["terms"]}
                 line.update(pd_errors(a, dq.T, dh.T, s))
                 print(json.dumps(line), flush=True)
-            h.set_option(zb.OPT_NS_FINISH, 0)
+            set_fast(False)
         elif w == "c4":
             import numpy as np
             rng = np.random.default_rng(1004)
@@ -180,18 +191,20 @@ def main(argv) -> int:
             du = torch.empty_like(da)
             ds = torch.empty(n, dtype=torch.float64, device="cuda")
             dv = torch.empty((n, n), dtype=torch.float64, device="cuda")
-            for algo in (1, 0):
+            for algo, fast in ((1, True), (1, False), (0, False)):
+                set_fast(fast)
                 ms = timed(lambda: zb.svd_dev(h, m, n, da.data_ptr(), m, du.data_ptr(), m, ds.data_ptr(),
                                               dv.data_ptr(), n, algo=algo, rk=8))
                 U, V = du.T, dv.T
                 line = {"workload": "c5 Zolo-SVD 16384x8192 kappa=1e10 clustered",
-                        "polar": "zolo-pd r=8" if algo else "qdwh", "ms": ms,
+                        "polar": ("zolo-pd r=8" + (" fast options" if fast else "")) if algo else "qdwh", "ms": ms,
                         "residual": float(torch.linalg.norm(a - (U * ds[None, :]) @ V.T) / torch.linalg.norm(a)),
                         "sv_err_rel_smax": float(torch.max(torch.abs(torch.sort(ds, descending=True).values - s))
                                                  / s[0]),
                         "orth_u": float(torch.linalg.norm(U.T @ U - eye(n)) / math.sqrt(n)),
                         "orth_v": float(torch.linalg.norm(V.T @ V - eye(n)) / math.sqrt(n))}
                 print(json.dumps(line), flush=True)
+            set_fast(False)
             del a, da, du, dv
             torch.cuda.empty_cache()
             h.release()
