@@ -217,6 +217,16 @@ __global__ void mirror_lower_kernel(int n, double* B, int64_t ldb) {
   }
 }
 
+__global__ void copy_upper_kernel(int n, const double* __restrict__ A, int64_t lda, double scale, double* B,
+                                  int64_t ldb) {
+  const int64_t total = static_cast<int64_t>(n) * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n), j = static_cast<int>(e / n);
+    B[i + static_cast<int64_t>(j) * ldb] = (i <= j) ? scale * A[i + static_cast<int64_t>(j) * lda] : 0.0;
+  }
+}
+
 __global__ void set_identity_kernel(int m, int n, double* Q, int64_t ldq, int64_t strideQ, double diag) {
   double* Qb = Q + blockIdx.y * strideQ;
   const int64_t total = static_cast<int64_t>(m) * n;
@@ -373,6 +383,12 @@ cudaError_t ns_prepare(int n, double* G, int64_t ldg, double* partial, double* e
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return reduce_sum(partial, blocks, err2, st);
+}
+
+cudaError_t copy_upper(int n, const double* A, int64_t lda, double scale, double* B, int64_t ldb, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  copy_upper_kernel<<<grid_for(static_cast<int64_t>(n) * n), TPB, 0, st>>>(n, A, lda, scale, B, ldb);
+  return cudaGetLastError();
 }
 
 cudaError_t mirror_lower(int n, double* B, int64_t ldb, cudaStream_t st) {

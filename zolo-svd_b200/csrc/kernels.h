@@ -69,6 +69,8 @@ cudaError_t combine_update(int m, int n, double* X, int64_t ldx, const double* Z
                            double* partial, double* err2, cudaStream_t st);
 // H = (B + B^T)/2 (in place on an n x n matrix).
 cudaError_t symmetrize(int n, double* B, int64_t ldb, cudaStream_t st);
+// B = scale * triu(A) (n x n; zero below the diagonal)
+cudaError_t copy_upper(int n, const double* A, int64_t lda, double scale, double* B, int64_t ldb, cudaStream_t st);
 // B = A^T
 cudaError_t transpose(int m, int n, const double* A, int64_t lda, double* B, int64_t ldb,
                       cudaStream_t st);

@@ -279,32 +279,48 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
 // Q = H_1 ... H_k applied to the identity, one 128-column block reflector at a time from the
 // last block: Q(rows, J:nq) -= V_B (T_B (V_B^T Q(rows, J:nq))).  Columns left of J are still
 // identity columns with their one above the block's rows, so V_B^T leaves them zero.
-void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq, bool top_tri) {
-  if (nq < n) nq = n;
+// C <- H_1 ... H_n C (the Q of geqrf applied from the left), one 128-column block reflector
+// at a time from the last: C(rows, cols) -= V_B (T_B (V_B^T C(rows, cols))).  from_diag: C
+// starts as the identity, so block J touches columns J .. ncols-1 only (left of J they are
+// identity columns with their one above the block's rows, which V_B^T leaves zero).
+static void apply_q_blocks(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat C, int ncols,
+                           bool from_diag, int batch, bool top_tri) {
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
   Mat VB{c.buf("qr_vb", static_cast<size_t>(ldv) * QB * batch), ldv, ldv * QB};
   Mat TB{c.buf("qr_tb", static_cast<size_t>(QB) * QB * batch), QB, static_cast<int64_t>(QB) * QB};
-  Mat WB{c.buf("qr_wb", static_cast<size_t>(QB) * nq * batch), QB, static_cast<int64_t>(QB) * nq};
-  Mat PB{c.buf("qr_pb", static_cast<size_t>(QB) * nq * batch), QB, static_cast<int64_t>(QB) * nq};
-  ck(set_identity(mtot, nq, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
-  c.stats.launches++;
+  Mat WB{c.buf("qr_wb", static_cast<size_t>(QB) * ncols * batch), QB, static_cast<int64_t>(QB) * ncols};
+  Mat PB{c.buf("qr_pb", static_cast<size_t>(QB) * ncols * batch), QB, static_cast<int64_t>(QB) * ncols};
   const int nblk = (n + QB - 1) / QB;
   for (int b = nblk - 1; b >= 0; --b) {
     const int J = b * QB;
     const int jbB = std::min(QB, n - J);
     const PanelRows R = panel_rows(mtot, m_top, top_tri, J, jbB);
-    const int nc = nq - J;
+    const int c0 = from_diag ? J : 0;
+    const int nc = ncols - c0;
     ck(extract_v(R.mp, jbB, W.at(J, J).p, W.ld, W.stride, VB.p, VB.ld, VB.stride, batch, c.stream(), R.split,
                  R.gap));
     c.stats.launches++;
     block_t(c, jbB, VB, R.mp, T + (J / PW) * PW * PW, strideT, TB, batch);
-    panel_vt_b(c, R, jbB, nc, VB, Q.at(J, J), WB, batch);
-    // P = T_B (V_B^T Q): T_B is upper triangular (k from the row)
+    panel_vt_b(c, R, jbB, nc, VB, C.at(J, c0), WB, batch);
+    // P = T_B (V_B^T C): T_B is upper triangular (k from the row)
     gemm(c, 0, 0, jbB, nc, jbB, 1.0, TB, WB, 0.0, PB, batch, nullptr, 0, 2);
-    panel_b_minus_vp(c, R, jbB, nc, VB, PB, Q.at(J, J), batch);
+    panel_b_minus_vp(c, R, jbB, nc, VB, PB, C.at(J, c0), batch);
   }
+}
+
+void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq, bool top_tri) {
+  if (nq < n) nq = n;
+  ck(set_identity(mtot, nq, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
+  c.stats.launches++;
+  apply_q_blocks(c, mtot, n, m_top, W, T, Q, nq, true, batch, top_tri);
+}
+
+void ormqr_left(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat C, int ncols, int batch,
+                bool top_tri) {
+  if (ncols <= 0) return;
+  apply_q_blocks(c, mtot, n, m_top, W, T, C, ncols, false, batch, top_tri);
 }
 
 }  // namespace zolo

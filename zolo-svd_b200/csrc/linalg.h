@@ -59,5 +59,8 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
 // (mpdorgqr.f / dorgqr with N >= K).
 void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q, int batch, int nq = -1,
            bool top_tri = false);
+// C (mtot x ncols) <- Q C with Q = H_1 ... H_n the reflectors of geqrf (dormqr 'L', 'N').
+void ormqr_left(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat C, int ncols, int batch,
+                bool top_tri = false);
 
 }  // namespace zolo

@@ -162,15 +162,17 @@ void q1q2t(Context& c, int m, int mp, int n, Mat Qf, Mat Z, int batch) {
 // With `pf`, X = (the matrix pf factors) / scale: Q_x is pf's Q and R_x = R / scale, and
 // d_sqrtc must already hold scale * sqrt(c_j) ([R/scale; sqrt(c) I] and [R; scale sqrt(c) I]
 // have the same Q factor).
+// s_only (with pf): Z receives S = sum_j w_j Q1'_j Q2'_j^T / FONE itself (n x n) and Q_x is
+// never formed: the caller keeps the iterate as X = Q_x Y and updates Y.
 void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx, Mat W, Mat Qf, Mat Z, double* tau,
                           double* T, const double* d_sqrtc, const double* hw, double fone, int rk,
-                          const Prefactored* pf = nullptr) {
+                          const Prefactored* pf = nullptr, bool s_only = false, int m_canon = -1) {
   const int64_t ldn = even(n);
   Mat Xq{c.buf("zq_x", static_cast<size_t>(ldx) * n), ldx, 0};
   Mat Qx{c.buf("zq_q", static_cast<size_t>(ldx) * n), ldx, 0};
   if (pf) {
     Xq = Mat{const_cast<double*>(pf->W), pf->ldw, 0};
-    orgqr(c, m, n, -1, Xq, pf->T, Qx, 1);
+    if (!s_only) orgqr(c, m, n, -1, Xq, pf->T, Qx, 1);
   } else {
     ck(scale_copy(m, n, 1.0, X, ldx, 0, Xq.p, Xq.ld, 0, 1, 0.0, c.stream()));
     c.stats.launches++;
@@ -186,18 +188,21 @@ void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx
   c.stats.launches++;
   geqrf(c, mtot, n, mt, Ws, tau, T, rk, true);
   orgqr(c, mtot, n, mt, Ws, T, Qs, rk, -1, true);
-  Mat S{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
+  const bool direct = pf && s_only;
+  Mat S = direct ? Mat{Z.p, Z.ld, 0} : Mat{c.buf("G", static_cast<size_t>(ldn) * n), ldn, 0};
   for (int b = 0; b < rk; ++b) {
     // S += w_b Q1'_b Q2'_b^T.  [R_x; sqrt(c) I] = Q'_b R_b gives Q1'_b = R_x R_b^{-1} and
     // Q2'_b = sqrt(c) R_b^{-1}, both upper triangular: entry (i, j) needs k >= max(i, j)
     const Mat Qb{Qs.p + b * Qs.stride, lds, 0};
     gemm(c, 0, 1, n, n, n, hw[b] / fone, Qb, Qb.at(mt, 0), b == 0 ? 0.0 : 1.0, S, 1, nullptr, 0, 3);
   }
-  gemm(c, 0, 0, m, n, n, 1.0, Qx, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
+  if (!direct) gemm(c, 0, 0, m, n, n, 1.0, Qx, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
   const double dm = m, dn = n;
-  const double executed = (pf ? 2.0 : 4.0) * dm * dn * dn - (pf ? 2.0 : 4.0) * dn * dn * dn / 3.0 +
-                          rk * (2.0 * dn * dn * dn) + 2.0 * dm * dn * dn;
-  c.stats.flops_exec_delta += executed - rk * (4.0 * dm * dn * dn + dn * dn * dn);
+  const double executed = direct ? rk * (2.0 * dn * dn * dn)
+                                 : (pf ? 2.0 : 4.0) * dm * dn * dn - (pf ? 2.0 : 4.0) * dn * dn * dn / 3.0 +
+                                       rk * (2.0 * dn * dn * dn) + 2.0 * dm * dn * dn;
+  const double dmc = m_canon >= 0 ? m_canon : m;  // rows of the reference's stack [X; sqrt(c) I]
+  c.stats.flops_exec_delta += executed - rk * (4.0 * dmc * dn * dn + dn * dn * dn);
 }
 
 // Finish of the polar iteration by FP64 Newton-Schulz steps X <- X (3I - X^T X)/2.
@@ -456,10 +461,26 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   c.stats.alpha = alpha;
   c.stats.beta = beta;
   EventTimer total(c.stream());
-  const int64_t ldx = even(m);
+  // Factored iterate (with the bounds' QR at hand and the shared QR form): X = Q_x Y with
+  // Q_x the Q of A/alpha = Q_x R, so X0 = A/(alpha beta) has Y0 = R/beta.  Every step keeps
+  // Q_x on the left (the QR of X is Q_x times the QR of Y; X^T X = Y^T Y; X S = Q_x (Y S)),
+  // so the iteration runs on the n x n Y; at the end Q = Q_x Y through the reflectors and
+  // H = sym(Q^T A) = sym(alpha R^T Y).  That saves forming Q_x, the m x n products with it
+  // and H's 2mn^2.
+  const bool factored = pf && c.zolo_shared_qr && !(sym == 'S' || sym == 's');
+  const int mx = factored ? n : m;  // rows of the iterate
+  const int64_t ldx = even(mx);
   double* X = c.buf("Xit", static_cast<size_t>(ldx) * n);
-  ck(scale_copy(m, n, 1.0 / (alpha * beta), dA, lda, 0, X, ldx, 0, 1, 0.0, c.stream()));
-  c.stats.launches++;
+  // R with its zeros below the diagonal (the reflectors live there), for H at the end
+  double* Rx = factored && dH ? c.buf("zf_r", static_cast<size_t>(even(n)) * n) : nullptr;
+  if (factored) {
+    ck(copy_upper(n, pf->W, pf->ldw, 1.0 / beta, X, ldx, c.stream()));
+    if (Rx) ck(copy_upper(n, pf->W, pf->ldw, 1.0, Rx, even(n), c.stream()));
+    c.stats.launches += 2;
+  } else {
+    ck(scale_copy(m, n, 1.0 / (alpha * beta), dA, lda, 0, X, ldx, 0, 1, 0.0, c.stream()));
+    c.stats.launches++;
+  }
 
   const double eps = eps_precision();
   const double tol = eps;
@@ -491,7 +512,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   // term plan (ZOLO_OPT_TERM_PLAN): needs the measured Newton-Schulz finish to end the loop;
   // its coefficients come from the complementary modulus (exact at any CON)
   const bool plan_terms = ns_finish && c.zolo_term_plan && c.zolo_chol_inverse && !left;
-  TermPlanner planner(rk, m, n, tol);
+  TermPlanner planner(rk, mx, n, tol);
   int planned = 0;
   // with the Newton-Schulz finish the loop ends at the measured check, not on ||X_{k+1} - X_k||
   while ((ns_finish || err > tol2) && it < maxit) {
@@ -505,7 +526,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     bool use_qr = plan_terms ? con > kConChol : (it == 0 || con > 1.0e3) && maxc > 3.0e2;
     bool z_summed = false;  // Z holds sum_j w_j Z_j / FONE already (one Z instead of r)
     if (!use_qr) {
-      gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
+      gemm(c, 1, 0, n, n, mx, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       if (ns_finish) {
         // G = X^T X is in hand: once X is within 0.1 of orthogonal (RMS of sigma^2 - 1),
         // the rest of the iteration is FP64 Newton-Schulz (the polar factor of X is that of A)
@@ -514,7 +535,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         const double e0 = std::sqrt(d2h(c, scal + 2) / n);
         // with the term plan: Newton-Schulz from the measured e0 only when cheaper than the plan
         if (e0 <= kNsEnter && (!plan_terms || planner.ns_cost(e0) <= planner.cost_from(con))) {
-          newton_schulz_finish(c, m, n, X, ldx, G, Z, e0, it);
+          newton_schulz_finish(c, mx, n, X, ldx, G, Z, e0, it);
           c.stats.ns_finish = 1;
           c.stats.ms_finish = tstep.stop();
           break;
@@ -544,15 +565,16 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         }
         ck(mirror_lower(n, S.p, S.ld, c.stream()));
         c.stats.launches++;
-        gemm(c, 0, 0, m, n, n, 1.0, Mat{X, ldx, 0}, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
+        gemm(c, 0, 0, mx, n, n, 1.0, Mat{X, ldx, 0}, S, 0.0, Mat{Z.p, Z.ld, 0}, 1);
         z_summed = true;
         c.stats.chol_iterations++;
         if (it < 16) c.stats.branch[it] = 2;
-        const double dm = m, dn = n;
-        c.stats.flops += dm * dn * dn + rk_it * (dn * dn * dn / 3.0 + 2.0 * dm * dn * dn);
-        c.stats.flops_exec_delta += rk_it * (dn * dn * dn - 2.0 * dm * dn * dn) + 2.0 * dm * dn * dn;
+        const double dm = m, dmx = mx, dn = n;
+        const double canonical = dm * dn * dn + rk_it * (dn * dn * dn / 3.0 + 2.0 * dm * dn * dn);
+        c.stats.flops += canonical;
+        c.stats.flops_exec_delta += 3.0 * dmx * dn * dn + rk_it * dn * dn * dn - canonical;
       } else {
-        spd_solve(c, m, n, X, ldx, Wc, Dz, Z, rk_it, left);
+        spd_solve(c, mx, n, X, ldx, Wc, Dz, Z, rk_it, left);
         for (int b = 0; b < rk_it; ++b) hv[16 + b] = -coeff[2 * rk_it + b];
         c.stats.chol_iterations++;
         if (it < 16) c.stats.branch[it] = 2;
@@ -571,7 +593,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       h2d(c, dvec, hv.data(), rk_it);
       for (int b = 0; b < rk_it; ++b) hv[16 + b] = -coeff[2 * rk_it + b] / std::sqrt(coeff[2 * b]);
       if (shared) {
-        zolo_terms_shared_qr(c, m, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk_it, pfi);
+        zolo_terms_shared_qr(c, mx, n, X, ldx, W, Qf, Z, tau, T, dvec, hv.data() + 16, fone, rk_it, pfi, factored,
+                             m);
       } else {
         ck(form_stack(m, mp, n, X, ldx, W.p, W.ld, W.stride, dvec, 0.0, rk_it, c.stream()));
         c.stats.launches++;
@@ -587,11 +610,11 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     }
     if (z_summed) {
       // Z already holds sum_j w_j Z_j / FONE
-      ck(combine_update(m, n, X, ldx, Z.p, Z.ld, 0, 1, 1.0 / fone, 1.0, nullptr, part, scal, c.stream()));
+      ck(combine_update(mx, n, X, ldx, Z.p, Z.ld, 0, 1, 1.0 / fone, 1.0, nullptr, part, scal, c.stream()));
     } else {
       for (int b = 0; b < rk_it; ++b) hv[16 + b] /= fone;
       h2d(c, dvec + 16, hv.data() + 16, rk_it);
-      ck(combine_update(m, n, X, ldx, Z.p, Z.ld, Z.stride, rk_it, 1.0 / fone, 0.0, dvec + 16, part, scal,
+      ck(combine_update(mx, n, X, ldx, Z.p, Z.ld, Z.stride, rk_it, 1.0 / fone, 0.0, dvec + 16, part, scal,
                         c.stream()));
     }
     c.stats.launches += 2;
@@ -610,6 +633,31 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   c.stats.ms_iter = ti.stop();
   c.stats.iterations = it;
   c.stats.last_err = err;
+  if (factored) {
+    // Q = Q_x Y: [Y; 0] through the reflectors of A/alpha = Q_x R
+    ck(set_identity(m, n, dQ, ldq, 0, 1, 0.0, c.stream()));
+    ck(scale_copy(n, n, 1.0, X, ldx, 0, dQ, ldq, 0, 1, 0.0, c.stream()));
+    c.stats.launches += 2;
+    ormqr_left(c, m, n, -1, Mat{const_cast<double*>(pf->W), pf->ldw, 0}, pf->T, Mat{dQ, ldq, 0}, n, 1);
+    const double dm = m, dn = n;
+    c.stats.flops_exec_delta += 4.0 * dm * dn * dn - 2.0 * dn * dn * dn;
+    if (dH) {
+      // H = sym(Q^T A) = sym(alpha Y^T R) = sym(alpha R^T Y): R^T is lower triangular (k up to the row)
+      EventTimer th(c.stream());
+      const int64_t ldh_i = even(n);
+      double* Hb = c.buf("Hbuf", static_cast<size_t>(ldh_i) * n);
+      gemm(c, 1, 0, n, n, n, alpha, Mat{Rx, even(n), 0}, Mat{X, ldx, 0}, 0.0, Mat{Hb, ldh_i, 0}, 1, nullptr, 0, 0,
+           nullptr, 1);
+      ck(symmetrize(n, Hb, ldh_i, c.stream()));
+      ck(scale_copy(n, n, 1.0, Hb, ldh_i, 0, dH, ldh, 0, 1, 0.0, c.stream()));
+      c.stats.launches += 2;
+      c.stats.flops += 2.0 * dm * dn * dn;
+      c.stats.flops_exec_delta += dn * dn * dn - 2.0 * dm * dn * dn;
+      c.stats.ms_h = th.stop();
+    }
+    c.stats.ms_total = total.stop();
+    return 0;
+  }
   ck(scale_copy(m, n, 1.0, X, ldx, 0, dQ, ldq, 0, 1, 0.0, c.stream()));
   c.stats.launches++;
   if (dH) {
