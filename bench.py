@@ -395,6 +395,8 @@ def run_gpu(args):
                        "l2": "inputs 512 MiB per matrix > 126 MB L2 (no flush needed)"},
             "accuracy": dict(acc_fast, iterations=st_fast["iterations"], ns_steps=st_fast["ns_steps"],
                              branches=st_fast["branches"], terms=st_fast["terms"]),
+            "phases_ms": {"bounds": st_fast["ms_bounds"], "iterations": st_fast["ms_step"],
+                          "finish": st_fast["ms_finish"], "h_and_q": st_fast["ms_h"]},
             "forms": {
                 "fast": {"s": t_ms / 1e3, "backward_error": acc_fast["backward_error"],
                          "orthogonality": acc_fast["orthogonality"], "branches": st_fast["branches"]},

@@ -53,7 +53,8 @@ typedef struct {
   double ms_total;     /* device time of the whole call (CUDA events)     */
   double ms_bounds;
   double ms_iter;
-  double ms_h;
+  double ms_h;         /* H (and, for zolo_polar_dev, Q = Q_x Y from the
+                          factored iterate) */
   double flops;        /* canonical FP64 flops of the executed steps      */
   int64_t launches;    /* kernels launched                                */
   double con[16];      /* per iteration: CON (Zolo) or c_k (QDWH)         */

@@ -634,6 +634,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   c.stats.iterations = it;
   c.stats.last_err = err;
   if (factored) {
+    EventTimer th(c.stream());  // ms_h covers Q = Q_x Y and H here
     // Q = Q_x Y: [Y; 0] through the reflectors of A/alpha = Q_x R
     ck(set_identity(m, n, dQ, ldq, 0, 1, 0.0, c.stream()));
     ck(scale_copy(n, n, 1.0, X, ldx, 0, dQ, ldq, 0, 1, 0.0, c.stream()));
@@ -643,7 +644,6 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     c.stats.flops_exec_delta += 4.0 * dm * dn * dn - 2.0 * dn * dn * dn;
     if (dH) {
       // H = sym(Q^T A) = sym(alpha Y^T R) = sym(alpha R^T Y): R^T is lower triangular (k up to the row)
-      EventTimer th(c.stream());
       const int64_t ldh_i = even(n);
       double* Hb = c.buf("Hbuf", static_cast<size_t>(ldh_i) * n);
       gemm(c, 1, 0, n, n, n, alpha, Mat{Rx, even(n), 0}, Mat{X, ldx, 0}, 0.0, Mat{Hb, ldh_i, 0}, 1, nullptr, 0, 0,
@@ -653,8 +653,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       c.stats.launches += 2;
       c.stats.flops += 2.0 * dm * dn * dn;
       c.stats.flops_exec_delta += dn * dn * dn - 2.0 * dm * dn * dn;
-      c.stats.ms_h = th.stop();
     }
+    c.stats.ms_h = th.stop();
     c.stats.ms_total = total.stop();
     return 0;
   }

@@ -148,8 +148,14 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
     const int buf = k & 1;
     // ---- gather: thread i < SLOT sums entry i over all CTAs (same order everywhere) ----
     if (tid < SLOT) {
+      // all remote loads are issued before the first add (one DSMEM latency, not CL of them);
+      // the sum keeps the rank order
+      double v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = (q < CL) ? cluster.map_shared_rank(&S.part[buf][0], q)[tid] : 0.0;
       double s = 0.0;
-      for (int q = 0; q < CL; ++q) s += cluster.map_shared_rank(&S.part[buf][0], q)[tid];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) s += v[q];
       S.sum[tid] = s;
     } else if (tid < SLOT + w) {
       const int owner = k / p.rows_per;
