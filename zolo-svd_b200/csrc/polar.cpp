@@ -97,8 +97,8 @@ class TermPlanner {
   double ns_cost(double e) const { return mu_ * kNsStep * ns_steps(e); }
 
  private:
-  static constexpr double kQrTerm = 2.6, kQrFixedPre = 7.3, kQrOfX = 3.9;
-  static constexpr double kChTerm = 1.2, kChFixed = 2.9, kNsStep = 2.95, kNsEntry = 1.0;
+  static constexpr double kQrTerm = 2.45, kQrFixedPre = 3.3, kQrOfX = 8.0;
+  static constexpr double kChTerm = 1.05, kChFixed = 4.3, kNsStep = 2.95, kNsEntry = 1.0;
   int rk_;
   double mu_, tol_, floor_e_;
   std::map<std::pair<double, int>, double> next_;
