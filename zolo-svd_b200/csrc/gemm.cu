@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(NT, C::MINB) dgemm_kernel(KParams kp) {
 
   int kb = 0, ke = p.K;
   if (p.kfrom_n) kb = min((p.kfrom_n == 1 ? n0 : (p.kfrom_n == 2 ? m0 : max(m0, n0))) / BK * BK, ke);
-  if (p.kto_m) ke = max(kb, min(ke, m0 + BM));
+  if (p.kto_m) ke = max(kb, min(ke, p.kto_m == 2 ? n0 + BN : m0 + BM));
   if (kp.splitk > 1) {
     const int span = ke - kb;
     int len = (span + kp.splitk - 1) / kp.splitk;

@@ -24,7 +24,8 @@ struct GemmArgs {
   int kfrom_n = 0;  // 1: op(B)(k,n) == 0 for k < n (op(B) lower triangular): skip those k;
                     // 2: op(A)(m,k) == 0 for k < m (op(A) upper triangular): skip those k;
                     // 3: both (k from max(row, column))
-  int kto_m = 0;    // 1: op(A)(m,k) == 0 for k > m (op(A) lower triangular): skip those k
+  int kto_m = 0;    // 1: op(A)(m,k) == 0 for k > m (op(A) lower triangular): skip those k;
+                    // 2: op(B)(k,n) == 0 for k > n (op(B) upper triangular): skip those k
   int splitk = 0;   // 0 = choose; 1 = off; >1 = number of K slices
 };
 

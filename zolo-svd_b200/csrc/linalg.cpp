@@ -68,7 +68,11 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
       const double nn = std::min(N, K);
       f = 2.0 * M * (static_cast<double>(N) * K - nn * (nn - 1.0) / 2.0 - (N - nn) * static_cast<double>(K));
     }
-    if (kto_m) {
+    if (kto_m == 2) {
+      // column j uses k <= j: sum over columns of min(K, j + 1)
+      const double nn = std::min(N, K);
+      f = 2.0 * M * (nn * (nn + 1.0) / 2.0 + (N - nn) * static_cast<double>(K));
+    } else if (kto_m) {
       // row i uses k <= i: sum over rows of min(K, i + 1)
       const double mm = std::min(M, K);
       f = 2.0 * N * (mm * (mm + 1.0) / 2.0 + (M - mm) * static_cast<double>(K));
@@ -109,6 +113,42 @@ void potrf(Context& c, int n, Mat A, int batch, int* dinfo, DiagInv D) {
     c.buf("potrf_tmp", static_cast<size_t>((n2 + 1) / 2 * 2) * n1 * batch);
   }
   potrf_rec(c, n, A, batch, dinfo, 0, D);
+}
+
+// Cholesky and the inverse of its factor together: with L11 and Y11 = L11^{-1} from the
+// first half, L21 = A21 Y11^T is one GEMM (no recursive triangular solve), then
+// A22 -= L21 L21^T, the second half, and Y21 = -Y22 (L21 Y11).  n^3/3 + n^3/3 flops, as
+// Cholesky plus triangular inverse, in about half the launches.
+static void potrf_inv_rec(Context& c, int n, Mat A, Mat Y, int batch, int* dinfo, int off, DiagInv D, Mat Tmp) {
+  if (n <= NB) {
+    Profiler::Rec rec;
+    if (c.prof.on) c.prof.begin(2, static_cast<double>(n) * n * n / 3.0 * batch, c.stream(), &rec);
+    ck(potrf_leaf(n, A.p, A.ld, A.stride, batch, dinfo, off, D.block(off / NB), D.stride, c.stream()));
+    if (c.prof.on) c.prof.end(rec, c.stream());
+    ck(scale_copy(n, n, 1.0, D.block(off / NB), NB, D.stride, Y.p, Y.ld, Y.stride, batch, 0.0, c.stream()));
+    c.stats.launches += 2;
+    return;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  potrf_inv_rec(c, n1, A, Y, batch, dinfo, off, D, Tmp);
+  // L21 = A21 Y11^T: Y11^T is upper triangular (k up to the column)
+  ck(scale_copy(n2, n1, 1.0, A.at(n1, 0).p, A.ld, A.stride, Tmp.p, Tmp.ld, Tmp.stride, batch, 0.0, c.stream()));
+  c.stats.launches++;
+  gemm(c, 0, 1, n2, n1, n1, 1.0, Tmp, Y, 0.0, A.at(n1, 0), batch, nullptr, 0, 0, nullptr, 2);
+  // A22 -= L21 L21^T (lower)
+  gemm(c, 0, 1, n2, n2, n1, -1.0, A.at(n1, 0), A.at(n1, 0), 1.0, A.at(n1, n1), batch, nullptr, 1, 0);
+  potrf_inv_rec(c, n2, A.at(n1, n1), Y.at(n1, n1), batch, dinfo, off + n1, D, Tmp);
+  // Y21 = -Y22 (L21 Y11): Y11 lower (k from the column), Y22 lower (k up to the row)
+  gemm(c, 0, 0, n2, n1, n1, 1.0, A.at(n1, 0), Y, 0.0, Tmp, batch, nullptr, 0, 1);
+  gemm(c, 0, 0, n2, n1, n2, -1.0, Y.at(n1, n1), Tmp, 0.0, Y.at(n1, 0), batch, nullptr, 0, 0, nullptr, 1);
+}
+
+void potrf_inv(Context& c, int n, Mat A, Mat Y, int batch, int* dinfo, DiagInv D) {
+  ck(set_identity(n, n, Y.p, Y.ld, Y.stride, batch, 0.0, c.stream()));  // zero upper triangle
+  c.stats.launches++;
+  const int64_t ldt = (n + 1) / 2 * 2;
+  Mat Tmp{c.buf("potrf_inv_tmp", static_cast<size_t>(ldt) * n * batch), ldt, ldt * n};
+  potrf_inv_rec(c, n, A, Y, batch, dinfo, 0, D, Tmp);
 }
 
 void diag_inverses(Context& c, int n, Mat L, int batch, DiagInv D) {

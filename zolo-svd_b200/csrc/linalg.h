@@ -32,6 +32,9 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
 // Lower Cholesky in place (n x n), recursive; info[b] > 0 on failure (LAPACK convention).
 // Dinv receives the inverses of the diagonal blocks of L (used by the solves below).
 void potrf(Context& c, int n, Mat A, int batch, int* dinfo, DiagInv Dinv);
+// Cholesky A = L L^T (lower, in place) and Y = L^{-1} (lower, upper triangle zero) together;
+// D receives the leaves' diagonal-block inverses, dinfo LAPACK INFO per batch entry.
+void potrf_inv(Context& c, int n, Mat A, Mat Y, int batch, int* dinfo, DiagInv D);
 // Dinv for a lower-triangular L that did not come from potrf.
 void diag_inverses(Context& c, int n, Mat L, int batch, DiagInv Dinv);
 // Y = X L^{-T}  (X m x n is destroyed; L's diagonal block k has inverse Dinv.block(k0 + k))

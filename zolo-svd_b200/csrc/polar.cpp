@@ -547,7 +547,14 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       ck(shift_lower(n, G.p, G.ld, Wc.p, Wc.ld, Wc.stride, dvec, rk_it, c.stream()));
       ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * rk_it, c.stream()));
       c.stats.launches += 2;
-      potrf(c, n, Wc, rk_it, dinfo, Dz);
+      // the explicit-inverse form takes the factors' inverses from the same recursion
+      Mat Y{nullptr, ldn, ldn * n};
+      if (inverse_form) {
+        Y.p = c.buf("zc_y", static_cast<size_t>(ldn) * n * rk_it);
+        potrf_inv(c, n, Wc, Y, rk_it, dinfo, Dz);
+      } else {
+        potrf(c, n, Wc, rk_it, dinfo, Dz);
+      }
       const int pinfo = read_info(c, dinfo, rk_it);
       if (pinfo != 0) {
         if (c.stats.info == 0) c.stats.info = pinfo;
@@ -555,8 +562,6 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       } else if (inverse_form) {
         // explicit form: S = sum_b w_b W_b^{-1}, W_b^{-1} = L_b^{-T} L_b^{-1}, then one Z = X S
         const double fone_c = zolo_fone(coeff.data(), rk_it);
-        Mat Y{c.buf("zc_y", static_cast<size_t>(ldn) * n * rk_it), ldn, ldn * n};
-        trtri_lower(c, n, Wc, Y, rk_it, Dz);
         Mat S{c.buf("zc_s", static_cast<size_t>(ldn) * n), ldn, 0};
         for (int b = 0; b < rk_it; ++b) {
           const double w = -coeff[2 * rk_it + b] / fone_c;
