@@ -8,7 +8,8 @@ profiler pointed at one case sees the same kernel configuration as the full
 solve (e.g. ``ncu -k regex:dgemm_kernel ... python kernel_cases.py --case gemm_nn``):
 
   gemm_nn      C = A B, M = N = K = n          (general DMMA GEMM, 128 x 128 tiles)
-  gemm_rank32  C -= A B, M = N = n, K = 32     (Householder trailing update, 64 x 64 tiles)
+  gemm_rank32  C -= A B, M = N = n, K = 32     (streaming rank-32 update kernel)
+  gemm_k128    C -= A B, M = N = n, K = 128    (block-reflector update, 64 x 64 tiles, C preloaded)
   gemm_m32     P = V^T W, M = 32, N = K = n    (panel projection, 32 x 64 tiles)
   syrk         lower(C) = A^T A, n x n          (Gram of the Cholesky form)
   geqrf        Householder QR of an n x n matrix (panel kernel + trailing GEMMs)
@@ -37,7 +38,7 @@ def load_pkg():
     return mod
 
 
-CASES = ("gemm_nn", "gemm_rank32", "gemm_m32", "syrk", "geqrf", "potrf")
+CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf")
 
 
 def main() -> int:
@@ -61,11 +62,13 @@ def main() -> int:
 
     lib = zb.lib()
     flops = 0.0
-    if args.case in ("gemm_nn", "gemm_rank32", "gemm_m32", "syrk"):
+    if args.case in ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk"):
         if args.case == "gemm_nn":
             M, N, K, ta, tri = n, n, n, b"N", 0
         elif args.case == "gemm_rank32":
             M, N, K, ta, tri = n, n, 32, b"N", 0
+        elif args.case == "gemm_k128":
+            M, N, K, ta, tri = n, n, 128, b"N", 0
         elif args.case == "gemm_m32":
             M, N, K, ta, tri = 32, n, n, b"T", 0
         else:
@@ -74,8 +77,8 @@ def main() -> int:
         b = randn(K, N)
         c = randn(M, N)
         lda = a.shape[1]
-        beta = -1.0 if args.case == "gemm_rank32" else 0.0
-        alpha = -1.0 if args.case == "gemm_rank32" else 1.0
+        beta = 1.0 if args.case in ("gemm_rank32", "gemm_k128") else 0.0
+        alpha = -1.0 if args.case in ("gemm_rank32", "gemm_k128") else 1.0
         flops = (1.0 if tri else 2.0) * M * N * K
 
         def run():
