@@ -426,3 +426,28 @@ def test_fast_form_all_options(m, n, kappa, plan):
     assert len(st["terms"]) == its and all(1 <= t <= 8 for t in st["terms"])
     if not plan:
         assert all(t == 8 for t in st["terms"])
+
+
+@pytest.mark.parametrize("m,n,kappa", [(330, 200, 1e12), (300, 300, 1e16), (257, 257, 1e4)])
+def test_term_plan_through_pzolopd1(m, n, kappa):
+    """The term plan on the PZOLOPD1 entry point (separate bounds, iterate not factored):
+    backward stable, the same polar factor as the reference steps, 1..rk terms."""
+    import torch
+    s = np.geomspace(1.0, 1.0 / kappa, n)
+    a, u, v = zo.make_matrix(n, s, 670 + m + n, m=m)
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=2)
+    for opt in (zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_TERM_PLAN):
+        h.set_option(opt, 1)
+    dq = torch.zeros_like(da)
+    dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    assert zb.pzolopd1_dev(h, "N", 8, m, n, al, be, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n) == 0
+    st = h.stats()
+    h.close()
+    q, hh = zb.device_to_colmajor(dq), zb.device_to_colmajor(dh)
+    check_pd(a, q, hh, n)
+    assert zo.backward_error(a, q, hh) <= 1e-13
+    assert np.linalg.norm(q - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
+    assert all(1 <= t <= 8 for t in st["terms"])
