@@ -451,3 +451,27 @@ def test_term_plan_through_pzolopd1(m, n, kappa):
     assert zo.backward_error(a, q, hh) <= 1e-13
     assert np.linalg.norm(q - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
     assert all(1 <= t <= 8 for t in st["terms"])
+
+
+@pytest.mark.parametrize("m,n", [(7, 5), (40, 33), (64, 64), (65, 65), (130, 1), (3, 3)])
+def test_fast_form_small_sizes(m, n):
+    """The fast form (factored iterate, term plan and the other cost options) at sizes below one
+    64-column leaf or one 128-column block, and with dH = NULL: backward stable, orthogonal Q."""
+    import torch
+    s = np.geomspace(1.0, 1e-6, n)
+    a, u, v = zo.make_matrix(n, s, 680 + m + n, m=m)
+    h = zb.Handle(0)
+    for opt in (zb.OPT_SHARED_QR, zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_BETA_FROB, zb.OPT_TERM_PLAN):
+        h.set_option(opt, 1)
+    da = zb.colmajor_to_device(a)
+    dq = torch.zeros_like(da)
+    dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    dq2 = torch.zeros_like(da)
+    torch.cuda.synchronize()
+    assert zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n) == 0
+    assert zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq2.data_ptr(), m, 0, 1) == 0  # no H
+    h.close()
+    q, hh, q2 = zb.device_to_colmajor(dq), zb.device_to_colmajor(dh), zb.device_to_colmajor(dq2)
+    check_pd(a, q, hh, n)
+    np.testing.assert_array_equal(q, q2)
+    assert np.linalg.norm(q - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * 1e6)
