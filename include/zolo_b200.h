@@ -148,6 +148,15 @@ int zolo_compute_coeff(double con, double tol, int rk, double* coeff);
  * accurate to ~1e-10 relative at any CON > 1, where Compute_Coeff's alpha = acos(1/CON) has a
  * relative error of ~1e-16 CON.  Used by ZOLO_OPT_TERM_PLAN.  No reference counterpart. */
 int zolo_compute_coeff_kp(double con, double tol, int rk, double* coeff);
+/* The term plan of ZOLO_OPT_TERM_PLAN from CON on (host only, no GPU): terms[k] and
+ * qr_form[k] (1 = QR form, 0 = Cholesky form) of each predicted Zolo-PD iteration for an
+ * m x n problem with at most rk terms, and *ns_steps, the predicted Newton-Schulz steps of
+ * the finish.  prefactored = 1 when the QR of X is at hand for the first iteration (as in
+ * zolo_polar_dev).  Returns the number of iterations (at most maxlen), -1 for bad
+ * arguments.  The solve itself re-plans before every iteration from the same model and
+ * enters the finish from the measured ||X^T X - I||.  No reference counterpart. */
+int zolo_plan_terms(double con, int rk, int m, int n, int prefactored, int* terms, int* qr_form, int maxlen,
+                    int* ns_steps);
 /* mellipke (Auxil_Zolo.f90:36-71) */
 void zolo_mellipke(double alpha, double tol, double* k, double* e);
 /* MELLIPJ (Auxil_Zolo.f90:73-128) */

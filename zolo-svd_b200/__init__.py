@@ -84,6 +84,8 @@ _SIGS = [
     ("zolo_set_option", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_compute_coeff_kp", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
+    ("zolo_plan_terms", C.c_int, [C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
     ("zolo_mellipke", None, [C.c_double, C.c_double, c_double_p, c_double_p]),
     ("zolo_mellipj", None, [C.c_double, C.c_double, C.c_double, c_double_p, c_double_p, c_double_p]),
     ("zolo_choosem", C.c_int, [C.c_double]),
@@ -194,6 +196,17 @@ def compute_coeff(con: float, tol: float, rk: int) -> np.ndarray:
     if r != 0:
         raise ZoloError("zolo_compute_coeff", r)
     return out
+
+
+def plan_terms(con: float, rk: int, m: int, n: int, prefactored: bool = True, maxlen: int = 16):
+    """The term plan from CON on: ([(terms, "QR" | "CH"), ...], predicted Newton-Schulz steps)."""
+    terms = (C.c_int * maxlen)()
+    qr = (C.c_int * maxlen)()
+    ns = C.c_int()
+    k = lib().zolo_plan_terms(con, rk, m, n, 1 if prefactored else 0, terms, qr, maxlen, C.byref(ns))
+    if k < 0:
+        raise ZoloError("zolo_plan_terms", k)
+    return [(terms[i], "QR" if qr[i] else "CH") for i in range(k)], ns.value
 
 
 def compute_coeff_kp(con: float, tol: float, rk: int) -> np.ndarray:

@@ -298,6 +298,11 @@ int zolo_compute_coeff(double con, double tol, int rk, double* coeff) {
   return 0;
 }
 
+int zolo_plan_terms(double con, int rk, int m, int n, int prefactored, int* terms, int* qr_form, int maxlen,
+                    int* ns_steps) {
+  return zolo::plan_terms(con, rk, m, n, prefactored != 0, terms, qr_form, maxlen, ns_steps);
+}
+
 int zolo_compute_coeff_kp(double con, double tol, int rk, double* coeff) {
   if (rk < 1 || rk > 8 || !coeff) return -3;
   if (!(con > 1.0) || !std::isfinite(con)) return -1;

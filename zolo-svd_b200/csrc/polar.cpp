@@ -95,6 +95,10 @@ class TermPlanner {
   double cost_from(double con) { return plan(con, false, 3, nullptr) - (con > kConChol ? 0.0 : mu_ * kNsEntry); }
   // Newton-Schulz steps from a measured e to the rounding floor
   double ns_cost(double e) const { return mu_ * kNsStep * ns_steps(e); }
+  // CON after an iteration with r terms (the coefficients of compute_coeff_kp)
+  double con_after(double con, int r) { return next_con(con, r); }
+  // predicted Newton-Schulz steps once CON is within the finish threshold
+  int finish_steps(double con) const { return ns_steps(2.0 * (con - 1.0)); }
 
  private:
   static constexpr double kQrTerm = 2.45, kQrFixedPre = 3.3, kQrOfX = 8.0;
@@ -675,6 +679,22 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   }
   c.stats.ms_total = total.stop();
   return 0;
+}
+
+int plan_terms(double con, int rk, int m, int n, bool prefactored, int* terms, int* qr_form, int maxlen,
+               int* ns_steps) {
+  if (rk < 1 || rk > 8 || m < n || n < 1 || !(con >= 1.0) || maxlen < 0) return -1;
+  TermPlanner planner(rk, m, n, eps_precision());
+  int len = 0;
+  while (2.0 * (con - 1.0) > 0.5 * kNsEnter && len < maxlen) {
+    const int r = planner.choose(con, prefactored && len == 0);
+    if (terms) terms[len] = r;
+    if (qr_form) qr_form[len] = con > kConChol ? 1 : 0;
+    con = planner.con_after(con, r);
+    ++len;
+  }
+  if (ns_steps) *ns_steps = planner.finish_steps(con);
+  return len;
 }
 
 int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq, double* dH,

@@ -46,6 +46,11 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
 // bounds (ZOLOPD form) + Zolo-PD + H in one call, the flow of the reference's driver
 // (test_zolodrv1.f90:167-198): the QR of A/alpha that gives beta is reused by the first
 // Zolo-PD iteration.  Returns INFO; alpha and beta are reported in the stats.
+// The term plan (ZOLO_OPT_TERM_PLAN) from CON on: terms[k] and qr_form[k] (1 = QR form) of
+// each predicted Zolo-PD iteration and the predicted Newton-Schulz steps; returns the number
+// of iterations (at most maxlen), or -1 for bad arguments.  Host only.
+int plan_terms(double con, int rk, int m, int n, bool prefactored, int* terms, int* qr_form, int maxlen,
+               int* ns_steps);
 int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq, double* dH,
                int64_t ldh);
 
