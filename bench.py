@@ -185,6 +185,17 @@ def cpu_baseline(n_full: int, n_s: int, rk: int, kappa: float) -> dict:
             "sample_seconds": t, "iterations": st.iterations}
 
 
+def max_over_ranks(dist, value: float, device: str) -> float:
+    """The slowest rank's time: every rank contributes its own device time (the bench's
+    N-GPU numbers are the max over ranks, never a wall clock)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -309,11 +320,7 @@ def run_gpu(args):
             launches += last["launches"]
         e1.record(stream)
         torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) / steps
-        if dist:
-            tt = torch.tensor([t], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(dist, e0.elapsed_time(e1) / steps, "cuda")
         return t, launches, last
 
     # ---- headline: the fast form ----
@@ -367,11 +374,7 @@ def run_gpu(args):
         e2e_step()
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1) / e2e_steps
-    if dist:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(dist, f0.elapsed_time(f1) / e2e_steps, "cuda")
 
     gk = [k for k in prof if k.startswith("dgemm")]
     g = {"ms": sum(prof[k]["ms"] for k in gk), "flops": sum(prof[k]["flops"] for k in gk),
