@@ -16,29 +16,42 @@ constexpr int PT = 256;
 constexpr int MAXE = (LEAF * (LEAF + 1) / 2 + PT - 1) / PT;  // lower-triangle elements per thread
 
 // x = l^{-1} for lower-triangular l (nb x nb in shared memory, ld LDS).
-// Column j of the inverse is owned by a group of 4 lanes that split every
-// dot product 4 ways; columns are independent, so only warp-level
-// synchronisation is needed.
+// Column j of the inverse is owned by a group of 4 lanes; lane q of the group keeps rows
+// q, q+4, ... of the column in registers and the substitution runs right-looking: at row i
+// the owning lane forms x_i = b_i / l_ii (one multiply by a reciprocal computed up front),
+// the group shares it by a shuffle and every lane updates its rows below i.  Columns are
+// independent, so only the 4-lane groups exchange data; the per-row work is independent
+// FMAs, not a dependent dot product.
 __device__ void tri_inverse_smem(int nb, const double* l, double* x) {
+  __shared__ double rdiag[LEAF];
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) rdiag[i] = 1.0 / l[i + i * LDS];
+  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j = warp * 8 + (lane >> 2);
   const int q = lane & 3;
-  const bool own = j < nb;
-  if (own) {
-    for (int i = q; i < nb; i += 4) x[i + j * LDS] = 0.0;
+  const int base = lane & ~3;
+  double b[LEAF / 4];
+#pragma unroll
+  for (int u = 0; u < LEAF / 4; ++u) b[u] = (q + 4 * u == j) ? 1.0 : 0.0;  // e_j
+#pragma unroll
+  for (int t = 0; t < LEAF / 4; ++t) {
+#pragma unroll
+    for (int qi = 0; qi < 4; ++qi) {
+      const int i = 4 * t + qi;
+      if (i < nb) {
+        double xi = (q == qi) ? b[t] * rdiag[i] : 0.0;
+        xi = __shfl_sync(0xffffffffu, xi, base | qi);
+        if (q == qi) b[t] = xi;
+#pragma unroll
+        for (int u = 0; u < LEAF / 4; ++u)
+          if (q + 4 * u > i && q + 4 * u < nb) b[u] -= l[q + 4 * u + i * LDS] * xi;
+      }
+    }
   }
-  __syncwarp();
-  if (own && q == 0) x[j + j * LDS] = 1.0 / l[j + j * LDS];
-  __syncwarp();
-  for (int i = 1; i < nb; ++i) {
-    const bool act = own && i > j;
-    double s = 0.0;
-    if (act)
-      for (int k = j + q; k < i; k += 4) s += l[i + k * LDS] * x[k + j * LDS];
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    if (act && q == 0) x[i + j * LDS] = -s / l[i + i * LDS];
-    __syncwarp();
+  if (j < nb) {
+#pragma unroll
+    for (int u = 0; u < LEAF / 4; ++u)
+      if (q + 4 * u < nb) x[q + 4 * u + j * LDS] = b[u];
   }
 }
 
