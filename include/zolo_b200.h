@@ -313,8 +313,10 @@ int zolo_formx2_dev(zolo_handle_t h, int m, int n, double fone, double* dX, int6
  * a device looks the array's address up (cudaGetSymbolAddress) and should be made
  * before any stream capture.  All calls share the scratch: calls that overlap on the
  * GPU race and must be serialised by the caller.  Synchronises `stream` before
- * returning.  Returns LAPACK INFO (> 0: not positive definite), -1 if n < 0 or
- * n > ZOLO_NOALLOC_MAX_N, -3 if lda < max(1,n), -1000 - cudaError on a CUDA error. */
+ * returning.  Any lda >= max(1,n) is accepted; dA must be 8-byte aligned.  Returns
+ * LAPACK INFO (> 0: not positive definite), -1 if n < 0 or n > ZOLO_NOALLOC_MAX_N,
+ * -2 if dA is null (n > 0), -3 if lda < max(1,n), -1000 - cudaError on a CUDA error
+ * (-1000 - cudaErrorMisalignedAddress for a dA that is not 8-byte aligned). */
 #define ZOLO_NOALLOC_MAX_N 1024
 int zolo_dpotrf_noalloc(int n, double* dA, int64_t lda, void* stream);
 

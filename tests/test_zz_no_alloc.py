@@ -58,3 +58,27 @@ def test_dpotrf_noalloc_rejects_oversize_and_reports_info():
     d = zb.colmajor_to_device(np.eye(n))
     torch.cuda.synchronize()
     assert lib.zolo_dpotrf_noalloc(n, d.data_ptr(), n, stream) == 0
+
+
+def test_dpotrf_noalloc_padded_leading_dimension():
+    """An odd order with lda > n (the padding rows are neither read as data nor written)."""
+    import torch
+    lib = zb.lib()
+    h = zb.Handle(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    n, lda = 257, 260
+    a = _spd(n, 77)
+    buf = np.full((lda, n), 5.0)
+    buf[:n] = a
+    d_new = zb.colmajor_to_device(buf)
+    d_ref = zb.colmajor_to_device(a)
+    torch.cuda.synchronize()
+    assert lib.zolo_dpotrf_dev(h.ptr, n, d_ref.data_ptr(), n) == 0
+    assert lib.zolo_dpotrf_noalloc(n, d_new.data_ptr(), lda, stream) == 0
+    got = zb.device_to_colmajor(d_new)
+    l_ref = np.tril(zb.device_to_colmajor(d_ref))
+    tol = 20 * n * zo.EPS * np.sqrt(np.abs(np.diag(a)).max())
+    assert np.allclose(np.tril(got[:n]), l_ref, rtol=0, atol=tol)
+    assert np.all(got[n:] == 5.0)
+    assert lib.zolo_dpotrf_noalloc(n, None, lda, stream) == -2
+    h.close()

@@ -30,12 +30,26 @@ using zolo::CudaFailure;
 
 constexpr int kCudaBase = -1000;
 
+// Makes the handle's device current for the call and restores the caller's current
+// device on every exit path.
+struct DeviceGuard {
+  int saved = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+    if (saved != dev) zolo::ck(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (saved >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != saved) cudaSetDevice(saved);
+  }
+};
+
 template <class F>
 int guarded(zolo_handle_t h, F&& f) {
   if (!h) return -999;
   std::lock_guard<std::mutex> lk(h->ctx.mu);
   try {
-    zolo::ck(cudaSetDevice(h->ctx.device()));
+    DeviceGuard dg(h->ctx.device());
     return f(h->ctx);
   } catch (const CudaFailure& e) {
     return kCudaBase - static_cast<int>(e.err);

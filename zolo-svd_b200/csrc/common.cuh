@@ -1,6 +1,8 @@
 // Shared device helpers for the FP64 kernels (sm_100a).
 #pragma once
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <cstdint>
 
 #define ZDEV __device__ __forceinline__
@@ -38,6 +40,33 @@ ZDEV void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]
 ZDEV double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Kernel attributes (cudaFuncSetAttribute) and device properties are per device: these
+// helpers apply / compute them once for each device the library launches on.
+constexpr int kMaxDevices = 64;
+template <class F>
+inline cudaError_t once_per_device(std::atomic<int> (&state)[kMaxDevices], F&& set) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return set();
+  if (state[dev].load(std::memory_order_acquire) == 1) return cudaSuccess;
+  e = set();
+  if (e == cudaSuccess) state[dev].store(1, std::memory_order_release);
+  return e;
+}
+// cache[device] holds compute() (a positive value) after the first call on that device.
+template <class F>
+inline int per_device_value(std::atomic<int> (&cache)[kMaxDevices], F&& compute) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return compute();
+  int v = cache[dev].load(std::memory_order_acquire);
+  if (v <= 0) {
+    v = compute();
+    cache[dev].store(v, std::memory_order_release);
+  }
   return v;
 }
 

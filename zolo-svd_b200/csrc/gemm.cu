@@ -326,8 +326,11 @@ __global__ void splitk_reduce_kernel(GemmArgs p, int splitk, const double* P, in
 
 template <class C, bool TA, bool TB, bool V16>
 cudaError_t launch_t(const KParams& kp, dim3 grid, cudaStream_t st) {
-  static cudaError_t attr = cudaFuncSetAttribute(dgemm_kernel<C, TA, TB, V16>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, C::smem(TA, TB));
+  static std::atomic<int> attr_set[kMaxDevices];
+  const cudaError_t attr = once_per_device(attr_set, [] {
+    return cudaFuncSetAttribute(dgemm_kernel<C, TA, TB, V16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                C::smem(TA, TB));
+  });
   if (attr != cudaSuccess) return attr;
   dgemm_kernel<C, TA, TB, V16><<<grid, NT, C::smem(TA, TB), st>>>(kp);
   return cudaGetLastError();
@@ -413,14 +416,13 @@ int choose_splitk(const GemmArgs& a, int sms) {
 }  // namespace
 
 int num_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+  static std::atomic<int> cache[kMaxDevices];
+  return per_device_value(cache, [] {
+    int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
+    return sms > 0 ? sms : 148;
+  });
 }
 
 size_t dgemm_splitk_bytes(const GemmArgs& a, int sms) {

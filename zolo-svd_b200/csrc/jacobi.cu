@@ -133,7 +133,9 @@ __global__ void __launch_bounds__(JT) jacobi_kernel(const JacobiLeaf* leaves, in
 cudaError_t jacobi_leaves(const JacobiLeaf* d_leaves, int count, int max_sweeps, int* d_sweeps, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   constexpr int smem = 2 * JN * JLD * 8;
-  static cudaError_t attr = cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  static std::atomic<int> attr_set[kMaxDevices];
+  const cudaError_t attr = once_per_device(
+      attr_set, [] { return cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); });
   if (attr != cudaSuccess) return attr;
   jacobi_kernel<<<count, JT, smem, st>>>(d_leaves, max_sweeps, d_sweeps);
   return cudaGetLastError();

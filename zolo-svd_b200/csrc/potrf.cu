@@ -167,8 +167,10 @@ cudaError_t potrf_leaf(int nb, double* A, int64_t lda, int64_t strideA, int batc
                        double* Dinv, int64_t strideD, cudaStream_t st) {
   if (nb <= 0 || batch <= 0) return cudaSuccess;
   if (nb > LEAF) return cudaErrorInvalidValue;
-  static cudaError_t attr = cudaFuncSetAttribute(potrf_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 SMEM_BYTES);
+  static std::atomic<int> attr_set[kMaxDevices];
+  const cudaError_t attr = once_per_device(attr_set, [] {
+    return cudaFuncSetAttribute(potrf_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  });
   if (attr != cudaSuccess) return attr;
   potrf_leaf_kernel<<<batch, PT, SMEM_BYTES, st>>>(nb, A, lda, strideA, info, info_offset, Dinv, strideD);
   return cudaGetLastError();
@@ -177,8 +179,10 @@ cudaError_t potrf_leaf(int nb, double* A, int64_t lda, int64_t strideA, int batc
 cudaError_t trtri_blocks(int n, const double* L, int64_t ldl, int64_t strideL, double* Dinv, int batch,
                          cudaStream_t st) {
   if (n <= 0 || batch <= 0) return cudaSuccess;
-  static cudaError_t attr = cudaFuncSetAttribute(trtri_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 SMEM_BYTES);
+  static std::atomic<int> attr_set[kMaxDevices];
+  const cudaError_t attr = once_per_device(attr_set, [] {
+    return cudaFuncSetAttribute(trtri_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  });
   if (attr != cudaSuccess) return attr;
   const int nblk = (n + LEAF - 1) / LEAF;
   trtri_blocks_kernel<<<dim3(nblk, batch), PT, SMEM_BYTES, st>>>(n, L, ldl, strideL, Dinv, nblk);

@@ -400,14 +400,13 @@ constexpr size_t shared_base() { return ((sizeof(PanelShared) + 15) / 16) * 16; 
 
 template <bool SMEM>
 cudaError_t set_attrs() {
-  static cudaError_t done = cudaErrorNotReady;
-  if (done == cudaErrorNotReady) {
-    done = cudaFuncSetAttribute(qr_panel_kernel<SMEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(shared_base() + SMEM_CHUNK_CAP + 64));
-    if (done == cudaSuccess)
-      done = cudaFuncSetAttribute(qr_panel_kernel<SMEM>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  }
-  return done;
+  static std::atomic<int> attr_set[kMaxDevices];
+  return once_per_device(attr_set, [] {
+    const cudaError_t e = cudaFuncSetAttribute(qr_panel_kernel<SMEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(shared_base() + SMEM_CHUNK_CAP + 64));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(qr_panel_kernel<SMEM>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  });
 }
 
 template <bool SMEM>
@@ -432,9 +431,9 @@ cudaError_t launch_panel(const PanelArgs& pa, int cl, int batch, size_t smem, cu
 // 16-CTA clusters are non-portable: use them only if the device can place one
 // with the largest shared-memory footprint; otherwise the portable 8.
 int max_cluster() {
-  static int mc = 0;
-  if (!mc) {
-    mc = 8;
+  static std::atomic<int> cache[kMaxDevices];
+  return per_device_value(cache, [] {
+    int mc = 8;
     if (set_attrs<true>() == cudaSuccess) {
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(16, 1, 1);
@@ -451,8 +450,8 @@ int max_cluster() {
       if (cudaOccupancyMaxActiveClusters(&n, qr_panel_kernel<true>, &cfg) == cudaSuccess && n > 0) mc = 16;
     }
     cudaGetLastError();
-  }
-  return mc;
+    return mc;
+  });
 }
 
 }  // namespace

@@ -234,12 +234,14 @@ cudaError_t rank_update(const GemmArgs& a, cudaStream_t st) {
   p.col_tiles = (a.N + UN - 1) / UN;
   p.total = static_cast<int64_t>(a.batch) * p.row_blocks * p.col_tiles;
   constexpr int csmem = CSTAGES * STAGE * static_cast<int>(sizeof(double));
-  static cudaError_t attr8 =
-      cudaFuncSetAttribute(rank_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem);
-  static cudaError_t attr16 =
-      cudaFuncSetAttribute(rank_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem);
-  if (attr8 != cudaSuccess) return attr8;
-  if (attr16 != cudaSuccess) return attr16;
+  static std::atomic<int> attr_set[kMaxDevices];
+  const cudaError_t attr = once_per_device(attr_set, [] {
+    const cudaError_t e =
+        cudaFuncSetAttribute(rank_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(rank_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, csmem);
+  });
+  if (attr != cudaSuccess) return attr;
   auto al16 = [](const void* ptr, int64_t ld) {
     return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && ld % 2 == 0;
   };
