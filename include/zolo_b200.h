@@ -83,9 +83,9 @@ const char* zolo_version(void);
 /* Per-kernel-class device timing with CUDA events on the launching streams
  * (0 = DMMA GEMM general shapes, 1 = Householder panel, 2 = Cholesky leaf,
  * 3 = GEMM M <= 32, 4 = GEMM N <= 64, 5 = GEMM rank-k K <= 64, 6 = GEMM lower
- * triangle).  While enabled, zolo_profile_read fills out[3*cls + 0..2] =
- * {launches, milliseconds, algorithmic flops} accumulated since the last reset
- * (out holds 21 doubles). */
+ * triangle, 7 = FP64 product emulated on the INT8 tensor cores).  While enabled,
+ * zolo_profile_read fills out[3*cls + 0..2] = {launches, milliseconds, algorithmic
+ * flops} accumulated since the last reset (out holds 24 doubles). */
 int zolo_profile_enable(zolo_handle_t handle, int on);
 /* Thread-block-cluster size the Householder panel kernel uses for an m x w panel on the
  * current device (negative when the rows do not fit in shared memory). */
@@ -278,6 +278,17 @@ int zolo_zoloeig_dev(zolo_handle_t h, int n, const double* dQ, int64_t ldq, cons
 int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
                    int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
                    int kfrom_n);
+/* C = alpha op(A) op(B) + beta C like zolo_dgemm_dev, with the FP64 products emulated on
+ * the INT8 tensor cores (tcgen05.mma kind::i8): each row of op(A) and column of op(B) is
+ * scaled by a power of two and split into `slices` (6, 7 or 8) signed 7-bit digit planes,
+ * the digit products are accumulated exactly in INT32 and recombined in FP64.  slices = 8
+ * gives FP64-level normwise accuracy.  Requires slices * 127^2 * k < 2^31 (k <= 16642 at 8)
+ * and finite inputs.  Returns 0, -i for a bad argument i, -1000-cudaError, or -2000-code
+ * when a pipeline wait of the kernel timed out (code 901..906).  No reference counterpart:
+ * the reference's products are ScaLAPACK PDGEMM in FP64 (zolochol.f90:88-89). */
+int zolo_ozgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
+                    int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
+                    int kfrom_n, int slices);
 /* Lower Cholesky in place (PDPOTRF 'L'); returns LAPACK INFO. */
 int zolo_dpotrf_dev(zolo_handle_t h, int n, double* dA, int64_t lda);
 /* Y = X L^{-T} (trans = 'T') or Y = X L^{-1} (trans = 'N'); X is overwritten (workspace). */

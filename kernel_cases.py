@@ -14,6 +14,8 @@ solve (e.g. ``ncu -k regex:dgemm_kernel ... python kernel_cases.py --case gemm_n
   syrk         lower(C) = A^T A, n x n          (Gram of the Cholesky form)
   geqrf        Householder QR of an n x n matrix (panel kernel + trailing GEMMs)
   potrf        Cholesky of an SPD n x n matrix  (leaf kernel + GEMMs)
+  oz_nn        C = A B, M = N = K = n, FP64 emulated on the INT8 tensor cores (--slices planes)
+  oz_syrk      lower(C) = A^T A, n x n, emulated (one splitting for both sides)
 
   python kernel_cases.py --case gemm_nn --n 4096 --reps 3
 """
@@ -25,20 +27,21 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(HERE, "zolo-svd_b200")
 
 
 def load_pkg():
     if "zolo_svd_b200" in sys.modules:
         return sys.modules["zolo_svd_b200"]
-    spec = importlib.util.spec_from_file_location("zolo_svd_b200", os.path.join(HERE, "__init__.py"),
-                                                  submodule_search_locations=[HERE])
+    spec = importlib.util.spec_from_file_location("zolo_svd_b200", os.path.join(PKG, "__init__.py"),
+                                                  submodule_search_locations=[PKG])
     mod = importlib.util.module_from_spec(spec)
     sys.modules["zolo_svd_b200"] = mod
     spec.loader.exec_module(mod)
     return mod
 
 
-CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf")
+CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf", "oz_nn", "oz_syrk")
 
 
 def main() -> int:
@@ -46,6 +49,7 @@ def main() -> int:
     ap.add_argument("--case", choices=CASES, required=True)
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--slices", type=int, default=8)
     args = ap.parse_args()
     import torch
     zb = load_pkg()
@@ -86,6 +90,19 @@ def main() -> int:
                                     c.data_ptr(), M, tri, 0)
             if rc:
                 raise zb.ZoloError("zolo_dgemm_dev", rc)
+    elif args.case in ("oz_nn", "oz_syrk"):
+        tri = 1 if args.case == "oz_syrk" else 0
+        ta = b"T" if tri else b"N"
+        a = randn(n, n)
+        b = a if tri else randn(n, n)
+        c = randn(n, n)
+        flops = (1.0 if tri else 2.0) * n ** 3
+
+        def run():
+            rc = lib.zolo_ozgemm_dev(h.ptr, ta, b"N", n, n, n, 1.0, a.data_ptr(), n, b.data_ptr(), n, 0.0,
+                                     c.data_ptr(), n, tri, 0, args.slices)
+            if rc:
+                raise zb.ZoloError("zolo_ozgemm_dev", rc)
     elif args.case == "geqrf":
         w0 = randn(n, n)
         w = torch.empty_like(w0)

@@ -29,13 +29,14 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(HERE, "zolo-svd_b200")
 
 
 def load_pkg():
     if "zolo_svd_b200" in sys.modules:
         return sys.modules["zolo_svd_b200"]
-    spec = importlib.util.spec_from_file_location("zolo_svd_b200", os.path.join(HERE, "__init__.py"),
-                                                  submodule_search_locations=[HERE])
+    spec = importlib.util.spec_from_file_location("zolo_svd_b200", os.path.join(PKG, "__init__.py"),
+                                                  submodule_search_locations=[PKG])
     mod = importlib.util.module_from_spec(spec)
     sys.modules["zolo_svd_b200"] = mod
     spec.loader.exec_module(mod)

@@ -117,6 +117,9 @@ _SIGS = [
     ("zolo_dgemm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double,
                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_int64,
                                  C.c_int, C.c_int]),
+    ("zolo_ozgemm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double,
+                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_int64,
+                                  C.c_int, C.c_int, C.c_int]),
     ("zolo_dpotrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
     ("zolo_dtrsm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                  C.c_int64, C.c_void_p, C.c_int64]),
@@ -146,7 +149,8 @@ OPT_NS_FINISH = 2
 OPT_CHOL_INVERSE = 3
 OPT_BETA_FROB = 4
 OPT_TERM_PLAN = 5
-PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri"]
+PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
+                   "ozgemm"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
 

@@ -528,6 +528,24 @@ int zolo_dgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int 
   });
 }
 
+int zolo_ozgemm_dev(zolo_handle_t h, char transa, char transb, int m, int n, int k, double alpha, const double* dA,
+                    int64_t lda, const double* dB, int64_t ldb, double beta, double* dC, int64_t ldc, int tri,
+                    int kfrom_n, int slices) {
+  if (m < 0) return -4;
+  if (n < 0) return -5;
+  if (k < 0) return -6;
+  if (slices < 6 || slices > 8) return -17;
+  if (tri && m != n) return -15;
+  if (!zolo::ozgemm_k_ok(slices, k)) return -6;
+  return guarded(h, [&](Context& c) {
+    zolo::ozgemm(c, upper(transa), upper(transb), m, n, k, alpha, zolo::Mat{const_cast<double*>(dA), lda, 0},
+                 zolo::Mat{const_cast<double*>(dB), ldb, 0}, beta, zolo::Mat{dC, ldc, 0}, 1, slices, tri, kfrom_n);
+    zolo::ck(cudaStreamSynchronize(c.stream()));
+    const int st = zolo::oz_status(c);
+    return st ? -2000 - st : 0;
+  });
+}
+
 int zolo_dpotrf_dev(zolo_handle_t h, int n, double* dA, int64_t lda) {
   return guarded(h, [&](Context& c) {
     int* dinfo = c.dinfo();

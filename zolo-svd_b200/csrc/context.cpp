@@ -131,4 +131,11 @@ double* Context::dscal() { return buf("__scal", 64); }
 double* Context::dpartial() { return buf("__partial", 4096); }
 int* Context::dinfo() { return ibuf("__info", 1024); }
 
+int* Context::oz_status_word() {
+  const bool fresh = bufs_.find("oz_status") == bufs_.end();
+  int* p = ibuf("oz_status", 1);
+  if (fresh) ck(cudaMemsetAsync(p, 0, sizeof(int), stream_));
+  return p;
+}
+
 }  // namespace zolo

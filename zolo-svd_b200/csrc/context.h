@@ -35,9 +35,10 @@ struct Stats {
 // Optional per-kernel-class timing with CUDA events recorded around launches on
 // their own stream: 0 = DMMA GEMM (general shapes, K > 64), 1 = Householder panel,
 // 2 = Cholesky leaf, 3 = GEMM with M <= 32, 4 = GEMM with N <= 64,
-// 5 = GEMM rank-k update (K <= 64), 6 = GEMM lower-triangle output.
+// 5 = GEMM rank-k update (K <= 64), 6 = GEMM lower-triangle output, 7 = FP64 product
+// emulated on the INT8 tensor cores (ozgemm).
 struct Profiler {
-  static constexpr int kClasses = 7;
+  static constexpr int kClasses = 8;
   bool on = false;
   struct Rec {
     cudaEvent_t a, b;
@@ -104,6 +105,7 @@ class Context {
   double* dscal();     // 64 doubles
   double* dpartial();  // 4096 doubles
   int* dinfo();        // 1024 ints
+  int* oz_status_word();  // status of the INT8-emulated products (zeroed when allocated)
 
  private:
   int device_;

@@ -42,6 +42,29 @@ size_t dgemm_splitk_bytes(const GemmArgs& a, int num_sms);
 bool rank_update_applies(const GemmArgs& a);
 cudaError_t rank_update(const GemmArgs& a, cudaStream_t st);
 
+// ---- FP64 products emulated on the INT8 tensor cores (ozaki.cu) ----
+// C = alpha op(A) op(B) + beta C (batched, tri / kfrom_n / kto_m as in GemmArgs; no
+// alpha_vec) from S = `slices` (6..8) signed 7-bit digit planes of each operand, products
+// accumulated exactly in INT32 (requires slices * 127^2 * K < 2^31, ozgemm_k_ok).
+// Workspace sizes from ozgemm_work_bytes.  Device status codes 901..906: a pipeline wait
+// timed out.
+struct OzWorkSizes {
+  size_t slice_a = 0, slice_b = 0;  // bytes of digit planes
+  size_t rows_a = 0, rows_b = 0;    // padded rows (one max and one exponent per row)
+};
+struct OzWork {
+  int8_t* sliceA = nullptr;
+  int8_t* sliceB = nullptr;
+  unsigned long long* maxA = nullptr;
+  unsigned long long* maxB = nullptr;
+  int* expA = nullptr;
+  int* expB = nullptr;
+  int* status = nullptr;
+};
+size_t ozgemm_work_bytes(const GemmArgs& a, int slices, OzWorkSizes* sz);
+bool ozgemm_k_ok(int slices, int K);
+cudaError_t ozgemm(const GemmArgs& a, int slices, const OzWork& w, cudaStream_t st, int sms);
+
 // ---- elementwise / reductions (elementwise.cu) ----
 // dst(i,j) = s * src(i,j) (+ d on the diagonal), batched.
 cudaError_t scale_copy(int m, int n, double s, const double* src, int64_t lds, int64_t strideS,

@@ -3,6 +3,7 @@
 #include "linalg.h"
 
 #include <algorithm>
+#include <string>
 
 namespace zolo {
 
@@ -82,6 +83,63 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   ck(dgemm(a, c.splitk(side), s));
   if (c.prof.on) c.prof.end(rec, s);
   c.stats.launches += need ? 2 : 1;
+}
+
+void ozgemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
+            int batch, int slices, int tri, int kfrom_n, cudaStream_t st, int kto_m) {
+  GemmArgs a;
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  a.transA = transA;
+  a.transB = transB;
+  a.A = A.p;
+  a.lda = A.ld;
+  a.strideA = A.stride;
+  a.B = B.p;
+  a.ldb = B.ld;
+  a.strideB = B.stride;
+  a.C = C.p;
+  a.ldc = C.ld;
+  a.strideC = C.stride;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.batch = batch;
+  a.tri = tri;
+  a.kfrom_n = kfrom_n;
+  a.kto_m = kto_m;
+  cudaStream_t s = st ? st : c.stream();
+  const bool side = s == c.side_stream() && s != c.stream();
+  const std::string pre = side ? "ozs_" : "oz_";
+  OzWorkSizes sz;
+  ozgemm_work_bytes(a, slices, &sz);
+  OzWork w;
+  w.sliceA = reinterpret_cast<int8_t*>(c.buf(pre + "sa", (sz.slice_a + 7) / 8));
+  w.sliceB = reinterpret_cast<int8_t*>(c.buf(pre + "sb", (sz.slice_b + 7) / 8));
+  unsigned long long* rows =
+      reinterpret_cast<unsigned long long*>(c.buf(pre + "rows", (sz.rows_a + sz.rows_b) * 3 / 2 + 2));
+  w.maxA = rows;
+  w.maxB = rows + sz.rows_a;
+  w.expA = reinterpret_cast<int*>(rows + sz.rows_a + sz.rows_b);
+  w.expB = w.expA + sz.rows_a;
+  w.status = c.oz_status_word();
+  Profiler::Rec rec;
+  if (c.prof.on) {
+    const double f = (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K;
+    c.prof.begin(7, f * batch, s, &rec);
+  }
+  ck(zolo::ozgemm(a, slices, w, s, num_sms()));
+  if (c.prof.on) c.prof.end(rec, s);
+  c.stats.launches += 3;
+}
+
+int oz_status(Context& c) {
+  int* d = c.oz_status_word();
+  int v = 0;
+  ck(cudaMemcpyAsync(&v, d, sizeof(int), cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  if (v) ck(cudaMemsetAsync(d, 0, sizeof(int), c.stream()));
+  return v;
 }
 
 static void potrf_rec(Context& c, int n, Mat A, int batch, int* dinfo, int off, DiagInv D) {

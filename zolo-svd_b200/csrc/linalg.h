@@ -29,6 +29,14 @@ inline int nblocks(int n) { return (n + kLeaf - 1) / kLeaf; }
 void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
           int batch, const double* alpha_vec = nullptr, int tri = 0, int kfrom_n = 0,
           cudaStream_t st = nullptr, int kto_m = 0);
+// The same product with the FP64 multiplications emulated on the INT8 tensor cores
+// (ozaki.cu): `slices` (6..8) digit planes per operand; no alpha_vec.  Runs on ctx.stream()
+// or `st`; the digit planes live in the context's workspace ("oz_*", or "ozs_*" on the side
+// stream).  A pipeline timeout is recorded in the context's oz status word (oz_status()).
+void ozgemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
+            int batch, int slices, int tri = 0, int kfrom_n = 0, cudaStream_t st = nullptr, int kto_m = 0);
+// Reads (and clears) the oz status word: 0, or the code of the first pipeline timeout.
+int oz_status(Context& c);
 // Lower Cholesky in place (n x n), recursive; info[b] > 0 on failure (LAPACK convention).
 // Dinv receives the inverses of the diagonal blocks of L (used by the solves below).
 void potrf(Context& c, int n, Mat A, int batch, int* dinfo, DiagInv Dinv);
