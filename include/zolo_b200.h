@@ -138,6 +138,18 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * ZOLO_OPT_CHOL_INVERSE (SYM = 'N'); otherwise rk terms.  zolo_stats_t.terms records the
  * counts.  No reference counterpart. */
 #define ZOLO_OPT_TERM_PLAN 5
+/* ZOLO_OPT_MIXED: 0 (default) = every matrix product on the FP64 tensor path (DMMA);
+ * 1 = the mixed form: the large products (K >= 256 and at least one wave of output tiles)
+ * of the Cholesky-form iterations, of the Newton-Schulz finish and of forming Q and H run
+ * on the INT8 tensor cores with the FP64 product emulated from ZOLO_OPT_MIXED_SLICES digit
+ * planes per operand (zolo_ozgemm_dev); the bounds and the QR-form iterations stay on the
+ * FP64 tensor path (their graded triangular factors need FP64's elementwise accuracy; the
+ * row/column-scaled emulation is accurate normwise).  With 8 planes the emulated product
+ * has FP64-level normwise accuracy.  The term plan uses the mixed form's measured costs.
+ * No reference counterpart (the reference multiplies with ScaLAPACK PDGEMM in FP64). */
+#define ZOLO_OPT_MIXED 6
+/* ZOLO_OPT_MIXED_SLICES: digit planes of the emulated products, 6..8 (default 8). */
+#define ZOLO_OPT_MIXED_SLICES 7
 int zolo_set_option(zolo_handle_t handle, int option, int value);
 
 /* ---- host scalar routines (no GPU needed) ---- */

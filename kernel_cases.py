@@ -16,6 +16,9 @@ solve (e.g. ``ncu -k regex:dgemm_kernel ... python kernel_cases.py --case gemm_n
   potrf        Cholesky of an SPD n x n matrix  (leaf kernel + GEMMs)
   oz_nn        C = A B, M = N = K = n, FP64 emulated on the INT8 tensor cores (--slices planes)
   oz_syrk      lower(C) = A^T A, n x n, emulated (one splitting for both sides)
+  oz_k128      C -= A B, M = N = n, K = 128, emulated (the block-reflector update shape)
+  oz_m512      P = V^T W, M = 512, N = K = n, emulated (four batched 128-row projections)
+  gemm_m512    the same on the DMMA GEMM
 
   python kernel_cases.py --case gemm_nn --n 4096 --reps 3
 """
@@ -41,7 +44,7 @@ def load_pkg():
     return mod
 
 
-CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf", "oz_nn", "oz_syrk")
+CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf", "oz_nn", "oz_syrk", "oz_k128", "oz_m512", "gemm_m512")
 
 
 def main() -> int:
@@ -90,6 +93,27 @@ def main() -> int:
                                     c.data_ptr(), M, tri, 0)
             if rc:
                 raise zb.ZoloError("zolo_dgemm_dev", rc)
+    elif args.case in ("oz_k128", "oz_m512", "gemm_m512"):
+        if args.case == "oz_k128":
+            M, N, K, ta, alpha, beta = n, n, 128, b"N", -1.0, 1.0
+        else:
+            M, N, K, ta, alpha, beta = 512, n, n, b"T", 1.0, 0.0
+        a = randn(K, M) if ta == b"T" else randn(M, K)
+        b = randn(K, N)
+        c = randn(M, N)
+        lda = a.shape[1]
+        flops = 2.0 * M * N * K
+        oz = args.case.startswith("oz")
+
+        def run():
+            if oz:
+                rc = lib.zolo_ozgemm_dev(h.ptr, ta, b"N", M, N, K, alpha, a.data_ptr(), lda, b.data_ptr(), K, beta,
+                                         c.data_ptr(), M, 0, 0, args.slices)
+            else:
+                rc = lib.zolo_dgemm_dev(h.ptr, ta, b"N", M, N, K, alpha, a.data_ptr(), lda, b.data_ptr(), K, beta,
+                                        c.data_ptr(), M, 0, 0)
+            if rc:
+                raise zb.ZoloError("gemm", rc)
     elif args.case in ("oz_nn", "oz_syrk"):
         tri = 1 if args.case == "oz_syrk" else 0
         ta = b"T" if tri else b"N"

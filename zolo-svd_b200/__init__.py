@@ -149,6 +149,8 @@ OPT_NS_FINISH = 2
 OPT_CHOL_INVERSE = 3
 OPT_BETA_FROB = 4
 OPT_TERM_PLAN = 5
+OPT_MIXED = 6
+OPT_MIXED_SLICES = 7
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
                    "ozgemm"]
 

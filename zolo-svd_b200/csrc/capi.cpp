@@ -257,6 +257,16 @@ int zolo_set_option(zolo_handle_t h, int option, int value) {
       c.zolo_term_plan = value != 0;
       return 0;
     }
+    if (option == ZOLO_OPT_MIXED) {
+      if (value < 0 || value > 1) return -3;
+      c.zolo_mixed = value;
+      return 0;
+    }
+    if (option == ZOLO_OPT_MIXED_SLICES) {
+      if (value < 6 || value > 8) return -3;
+      c.oz_slices = value;
+      return 0;
+    }
     return -1;
   });
 }

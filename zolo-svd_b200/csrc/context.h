@@ -100,6 +100,13 @@ class Context {
   int zolo_beta_frob = 0;
   // Zolo-PD term counts: 0 = rk in every iteration, 1 = planned per iteration (r <= rk) by cost.
   int zolo_term_plan = 0;
+  // Mixed form: 0 = every product on the FP64 DMMA GEMM; 1 = the large products of the
+  // Cholesky iterations, the Newton-Schulz finish and Q, H run on the INT8-emulated GEMM
+  // (ozgemm, oz_slices digit planes); the bounds and the QR iterations stay on DMMA.
+  int zolo_mixed = 0;
+  int oz_slices = 8;
+  // digit planes of the products gemm() routes to ozgemm right now (0 = none); set by OzScope
+  int oz_active = 0;
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles
@@ -113,6 +120,15 @@ class Context {
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   std::map<std::string, std::pair<void*, size_t>> bufs_;
   Scratch splitk_, splitk_side_;
+};
+
+// Routes the large products of gemm() to the INT8-emulated GEMM while in scope (when the
+// handle's mixed form is on), and restores the previous routing on exit.
+struct OzScope {
+  Context& c;
+  int saved;
+  OzScope(Context& ctx, bool on) : c(ctx), saved(ctx.oz_active) { c.oz_active = on ? c.oz_slices : 0; }
+  ~OzScope() { c.oz_active = saved; }
 };
 
 }  // namespace zolo

@@ -20,8 +20,28 @@ int split_point(int n) {
 }
 }  // namespace
 
+namespace {
+// Products the INT8-emulated GEMM takes while an OzScope is active: long enough K for its
+// tile pipeline and at least one wave of 128 x 64 output tiles on the GPU.
+constexpr int kOzMinK = 256;
+bool oz_eligible(int M, int N, int K, int batch, int tri) {
+  if (K < kOzMinK || M <= 0 || N <= 0) return false;
+  const int64_t tm = (M + 127) / 128, tn = (N + 63) / 64;
+  int64_t tiles = tm * tn;
+  if (tri) {
+    tiles = 0;
+    for (int64_t i = 0; i < tm; ++i) tiles += std::min<int64_t>(tn, 2 * i + 2);
+  }
+  return tiles * batch >= num_sms();
+}
+}  // namespace
+
 void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha, Mat A, Mat B, double beta, Mat C,
           int batch, const double* alpha_vec, int tri, int kfrom_n, cudaStream_t st, int kto_m) {
+  if (c.oz_active && !alpha_vec && oz_eligible(M, N, K, batch, tri)) {
+    ozgemm(c, transA, transB, M, N, K, alpha, A, B, beta, C, batch, c.oz_active, tri, kfrom_n, st, kto_m);
+    return;
+  }
   GemmArgs a;
   a.M = M;
   a.N = N;
@@ -108,6 +128,18 @@ void ozgemm(Context& c, int transA, int transB, int M, int N, int K, double alph
   a.tri = tri;
   a.kfrom_n = kfrom_n;
   a.kto_m = kto_m;
+  if (!ozgemm_k_ok(slices, K)) {
+    // exact INT32 accumulation bounds K: run K in chunks, accumulating into C (the
+    // triangular k-skips refer to the whole K range and are dropped; zeros stay zeros)
+    const int kc = 16384;
+    for (int k0 = 0; k0 < K; k0 += kc) {
+      const int kk = std::min(kc, K - k0);
+      const Mat Ak{A.p + (transA ? k0 : static_cast<int64_t>(k0) * A.ld), A.ld, A.stride};
+      const Mat Bk{B.p + (transB ? static_cast<int64_t>(k0) * B.ld : k0), B.ld, B.stride};
+      ozgemm(c, transA, transB, M, N, kk, alpha, Ak, Bk, k0 == 0 ? beta : 1.0, C, batch, slices, tri, 0, st, 0);
+    }
+    return;
+  }
   cudaStream_t s = st ? st : c.stream();
   const bool side = s == c.side_stream() && s != c.stream();
   const std::string pre = side ? "ozs_" : "oz_";

@@ -63,6 +63,14 @@ struct EventTimer {
 
 int npanels(int n) { return (n + 31) / 32; }
 
+// With the mixed form on: 0, or -2000 - code when a pipeline wait of an INT8-emulated product
+// timed out during the solve (its results are then not to be used).
+int mixed_status(Context& c) {
+  if (!c.zolo_mixed) return 0;
+  const int st = oz_status(c);
+  return st ? -2000 - st : 0;
+}
+
 // Newton-Schulz finish of Zolo-PD (ZOLO_OPT_NS_FINISH): entry threshold on
 // ||X^T X - I||_F / sqrt(n) and the cap on the number of steps
 constexpr double kNsEnter = 0.1;
@@ -82,9 +90,21 @@ constexpr int kNsMaxSteps = 12;
 constexpr double kConChol = 12.0;
 class TermPlanner {
  public:
-  TermPlanner(int rk, int m, int n, double tol) : rk_(rk), mu_(static_cast<double>(m) / n), tol_(tol) {
+  // `mixed`: the Cholesky iterations and Newton-Schulz steps run their products on the
+  // INT8-emulated GEMM (measured at n = 8192: a Cholesky iteration 39 ms + 11.5 ms per term,
+  // a Newton-Schulz step 27 ms, the finish's first check 8 ms; 17 ms per unit)
+  TermPlanner(int rk, int m, int n, double tol, bool mixed = false)
+      : rk_(rk), mu_(static_cast<double>(m) / n), tol_(tol) {
     floor_e_ = std::max(1e-14, 0.5 * eps_precision() * std::sqrt(static_cast<double>(m)));
+    if (mixed) {
+      ch_term_ = 0.68;
+      ch_fixed_ = 2.3;
+      ns_step_ = 1.58;
+      ns_entry_ = 0.48;
+    }
   }
+  // the plan from CON is the finish itself (no further iteration predicted)
+  bool predicts_finish(double con) const { return 2.0 * (con - 1.0) <= 0.5 * kNsEnter; }
   // terms for the iteration at CON = con; `prefactored`: the QR of X is at hand (first iteration)
   int choose(double con, bool prefactored) {
     int first = rk_;
@@ -92,9 +112,9 @@ class TermPlanner {
     return first;
   }
   // cost of the cheapest plan from CON at a Cholesky iteration whose Gram is already formed
-  double cost_from(double con) { return plan(con, false, 3, nullptr) - (con > kConChol ? 0.0 : mu_ * kNsEntry); }
+  double cost_from(double con) { return plan(con, false, 3, nullptr) - (con > kConChol ? 0.0 : mu_ * ns_entry_); }
   // Newton-Schulz steps from a measured e to the rounding floor
-  double ns_cost(double e) const { return mu_ * kNsStep * ns_steps(e); }
+  double ns_cost(double e) const { return mu_ * ns_step_ * ns_steps(e); }
   // CON after an iteration with r terms (the coefficients of compute_coeff_kp)
   double con_after(double con, int r) { return next_con(con, r); }
   // predicted Newton-Schulz steps once CON is within the finish threshold
@@ -102,7 +122,7 @@ class TermPlanner {
 
  private:
   static constexpr double kQrTerm = 2.45, kQrFixedPre = 3.3, kQrOfX = 8.0;
-  static constexpr double kChTerm = 1.05, kChFixed = 4.3, kNsStep = 2.95, kNsEntry = 1.0;
+  double ch_term_ = 1.05, ch_fixed_ = 4.3, ns_step_ = 2.95, ns_entry_ = 1.0;
   int rk_;
   double mu_, tol_, floor_e_;
   std::map<std::pair<double, int>, double> next_;
@@ -127,13 +147,13 @@ class TermPlanner {
   }
   double plan(double con, bool prefactored, int depth, int* first) {
     const double e = 2.0 * (con - 1.0);
-    if (e <= 0.5 * kNsEnter) return mu_ * (kNsEntry + ns_steps(e) * kNsStep);
+    if (e <= 0.5 * kNsEnter) return mu_ * (ns_entry_ + ns_steps(e) * ns_step_);
     if (depth == 0) return 1e300;
     const bool qr = con > kConChol;
-    const double fixed = qr ? mu_ * (kQrFixedPre + (prefactored ? 0.0 : kQrOfX)) : mu_ * kChFixed;
+    const double fixed = qr ? mu_ * (kQrFixedPre + (prefactored ? 0.0 : kQrOfX)) : mu_ * ch_fixed_;
     double best = 1e300;
     for (int r = 1; r <= rk_; ++r) {
-      const double here = fixed + r * (qr ? kQrTerm : kChTerm);
+      const double here = fixed + r * (qr ? kQrTerm : ch_term_);
       if (here >= best) break;  // the cost of this iteration grows with r
       const double tot = here + plan(next_con(con, r), false, depth - 1, nullptr);
       if (tot < best) {
@@ -397,6 +417,7 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
     double akk, bkk;
     bool use_qr = ckk > 100.0;
     if (!use_qr) {
+      OzScope mixed_ch(c, c.zolo_mixed >= 1);  // the mixed form's products of this Cholesky step
       gemm(c, 1, 0, n, n, m, ckk, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       ck(add_diag(n, G.p, G.ld, 1.0, c.stream()));
       ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
@@ -448,11 +469,12 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
   c.stats.launches++;
   if (dH) {
     EventTimer th(c.stream());
+    OzScope mixed_h(c, c.zolo_mixed >= 1);
     form_h(c, m, n, X, ldx, Ain, ldx, dH, ldh);
     c.stats.ms_h = th.stop();
   }
   c.stats.ms_total = total.stop();
-  return 0;
+  return mixed_status(c);
 }
 
 int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double beta, const double* dA, int64_t lda,
@@ -516,7 +538,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   // term plan (ZOLO_OPT_TERM_PLAN): needs the measured Newton-Schulz finish to end the loop;
   // its coefficients come from the complementary modulus (exact at any CON)
   const bool plan_terms = ns_finish && c.zolo_term_plan && c.zolo_chol_inverse && !left;
-  TermPlanner planner(rk, mx, n, tol);
+  TermPlanner planner(rk, mx, n, tol, c.zolo_mixed >= 1);
   int planned = 0;
   // with the Newton-Schulz finish the loop ends at the measured check, not on ||X_{k+1} - X_k||
   while ((ns_finish || err > tol2) && it < maxit) {
@@ -530,6 +552,8 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     bool use_qr = plan_terms ? con > kConChol : (it == 0 || con > 1.0e3) && maxc > 3.0e2;
     bool z_summed = false;  // Z holds sum_j w_j Z_j / FONE already (one Z instead of r)
     if (!use_qr) {
+      // the mixed form's products of the Cholesky iteration (and of the finish entered here)
+      OzScope mixed_ch(c, c.zolo_mixed >= 1);
       gemm(c, 1, 0, n, n, mx, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
       if (ns_finish) {
         // G = X^T X is in hand: once X is within 0.1 of orthogonal (RMS of sigma^2 - 1),
@@ -538,7 +562,10 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
         c.stats.launches += 2;
         const double e0 = std::sqrt(d2h(c, scal + 2) / n);
         // with the term plan: Newton-Schulz from the measured e0 only when cheaper than the plan
-        if (e0 <= kNsEnter && (!plan_terms || planner.ns_cost(e0) <= planner.cost_from(con))) {
+        // (the plan's prediction can be reached only to rounding: when it predicts the finish,
+        // the measured e0 decides the steps)
+        if (e0 <= kNsEnter &&
+            (!plan_terms || planner.predicts_finish(con) || planner.ns_cost(e0) <= planner.cost_from(con))) {
           newton_schulz_finish(c, mx, n, X, ldx, G, Z, e0, it);
           c.stats.ns_finish = 1;
           c.stats.ms_finish = tstep.stop();
@@ -642,6 +669,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   c.stats.ms_iter = ti.stop();
   c.stats.iterations = it;
   c.stats.last_err = err;
+  OzScope mixed_h(c, c.zolo_mixed >= 1);  // forming Q and H
   if (factored) {
     EventTimer th(c.stream());  // ms_h covers Q = Q_x Y and H here
     // Q = Q_x Y: [Y; 0] through the reflectors of A/alpha = Q_x R
@@ -665,7 +693,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     }
     c.stats.ms_h = th.stop();
     c.stats.ms_total = total.stop();
-    return 0;
+    return mixed_status(c);
   }
   ck(scale_copy(m, n, 1.0, X, ldx, 0, dQ, ldq, 0, 1, 0.0, c.stream()));
   c.stats.launches++;
@@ -678,7 +706,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     c.stats.ms_h = th.stop();
   }
   c.stats.ms_total = total.stop();
-  return 0;
+  return mixed_status(c);
 }
 
 int plan_terms(double con, int rk, int m, int n, bool prefactored, int* terms, int* qr_form, int maxlen,
