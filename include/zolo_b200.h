@@ -150,7 +150,21 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
 #define ZOLO_OPT_MIXED 6
 /* ZOLO_OPT_MIXED_SLICES: digit planes of the emulated products, 6..8 (default 8). */
 #define ZOLO_OPT_MIXED_SLICES 7
+/* ZOLO_OPT_OWN_BOUNDS: 0 (default) = zolo_pzolopd1 / pzolopd1_ / zolo_pzolopd1_dev scale A
+ * by the caller's ALPHA and BETA, as the reference does (pzolopd1.f90:280-291); 1 = they
+ * compute ALPHA = ||A||_F and BETA from the QR of A/ALPHA (ZOLO_OPT_BETA_FROB form) and reuse
+ * that QR in the first iteration (the zolo_polar_dev flow).  The polar factor does not depend
+ * on the scaling of A, so Q is the same to rounding; SYM = 'S' keeps the caller's values.
+ * The caller still passes ALPHA, BETA > 0 (checked as before).  No reference counterpart. */
+#define ZOLO_OPT_OWN_BOUNDS 8
+/* The default handle (used by the reference-named host-array entry points) reads its options
+ * from the environment when it is created, so an unchanged Fortran driver selects them:
+ * ZOLO_FAST=1 sets ZOLO_OPT_SHARED_QR, _NS_FINISH, _CHOL_INVERSE, _BETA_FROB, _TERM_PLAN and
+ * _OWN_BOUNDS to 1; ZOLO_OPT_<NAME>=<integer> (e.g. ZOLO_OPT_MIXED=1) sets one option and
+ * overrides ZOLO_FAST; ZOLO_DEVICE=<ordinal> picks the GPU.  Invalid values are ignored. */
 int zolo_set_option(zolo_handle_t handle, int option, int value);
+/* Current value of an option of a handle in *value; -1 for an unknown option. */
+int zolo_get_option(zolo_handle_t handle, int option, int* value);
 
 /* ---- host scalar routines (no GPU needed) ---- */
 /* Compute_Coeff (Auxil_Zolo.f90:165-200): coeff[0:2rk] = c_i, coeff[2rk:3rk] = -a_i. */

@@ -141,3 +141,27 @@ def test_fortran_symbol_query_path():
     assert info.value == 0
     assert work[0] == max(5 * n + 4 + 1, 2 * n * n)
     assert work[1] == max(4 * (3 * n + 4) + 1, n * n)
+
+
+def test_fortran_interface_module_matches_header():
+    """include/zolo_b200.f90 binds only exported C names, with the header's option values and
+    the argument counts of the C prototypes (no Fortran compiler here: checked as text)."""
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    f90 = open(os.path.join(root, "include", "zolo_b200.f90")).read()
+    hdr = open(os.path.join(root, "include", "zolo_b200.h")).read()
+    lib = zb.lib()
+    binds = re.findall(r'(?:subroutine|function)\s+(\w+)\(([^)]*)\)[^\n]*?(?:&\s*\n[^\n]*?)?bind\(C, name="(\w+)"\)',
+                       f90)
+    assert len(binds) >= 12
+    for fname, args, cname in binds:
+        assert fname == cname
+        assert hasattr(lib, cname), cname
+        proto = re.search(r"\b" + cname + r"\(([^;]*)\);", hdr)
+        assert proto, cname
+        n_c = len([x for x in proto.group(1).split(",") if x.strip()])
+        n_f = len([x for x in args.replace("&", "").split(",") if x.strip()])
+        assert n_c == n_f, (cname, n_c, n_f)
+    for name, val in re.findall(r"integer\(c_int\), parameter :: (ZOLO_OPT_\w+) = (\d+)", f90):
+        assert re.search(r"#define " + name + r" " + val + r"\b", hdr), name

@@ -82,6 +82,7 @@ _SIGS = [
     ("zolo_panel_cluster_size", C.c_int, [C.c_int, C.c_int]),
     ("zolo_profile_read", C.c_int, [C.c_void_p, c_double_p, C.c_int]),
     ("zolo_set_option", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("zolo_get_option", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("zolo_compute_coeff", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_compute_coeff_kp", C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p]),
     ("zolo_plan_terms", C.c_int, [C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
@@ -151,6 +152,7 @@ OPT_BETA_FROB = 4
 OPT_TERM_PLAN = 5
 OPT_MIXED = 6
 OPT_MIXED_SLICES = 7
+OPT_OWN_BOUNDS = 8
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
                    "ozgemm"]
 
@@ -309,6 +311,39 @@ def pzolopd1(sym: str, rk: int, a: np.ndarray, alpha: float, beta: float, polar:
     return q, info.value
 
 
+def pzolopd_f77(sym: str, rk: int, m: int, n: int, alpha: float, beta: float, a_ptr: int, lda: int, q_ptr: int,
+                ldq: int, routine: str = "pzolopd1_", nb: int = 64) -> int:
+    """PZOLOPD1 / PZOLOPD2 through the gfortran-mangled symbol, as an unchanged Fortran driver
+    calls it (test_zolodrv1.f90:198): every argument by reference, hidden CHARACTER lengths
+    last, host arrays at raw addresses (column-major, leading dimensions lda, ldq), the
+    library's default handle (options from the environment).  Returns INFO."""
+    f = getattr(lib(), routine)
+    f.restype = None
+    da = _desc(m, n, nb, lda)
+    dq = _desc(m, n, nb, ldq)
+    iv = lambda v: C.byref(C.c_int(v))
+    info = C.c_int(0)
+    f(C.c_char_p(sym.encode()[:1]), iv(rk), iv(m), iv(n), C.byref(C.c_double(alpha)), C.byref(C.c_double(beta)),
+      C.c_void_p(a_ptr), iv(1), iv(1), da.ctypes.data_as(c_int_p), C.c_void_p(q_ptr), iv(1), iv(1),
+      dq.ctypes.data_as(c_int_p), C.byref(info), C.c_char_p(b"N"), C.c_size_t(1), C.c_size_t(1))
+    return info.value
+
+
+class DefaultHandle:
+    """The library's default handle: the one the reference-named host-array entry points use,
+    created on first use with its options read from the environment (ZOLO_FAST,
+    ZOLO_OPT_<NAME>, ZOLO_DEVICE).  Never destroyed from here."""
+
+    def __init__(self):
+        self.ptr = C.c_void_p()
+        r = lib().zolo_default_handle(C.byref(self.ptr))
+        if r != 0:
+            raise ZoloError("zolo_default_handle", r)
+
+    get_option = lambda self, option: Handle.get_option(self, option)
+    stats = lambda self: Handle.stats(self)
+
+
 # ---------------------------------------------------------------------------
 # device-pointer API
 # ---------------------------------------------------------------------------
@@ -353,6 +388,13 @@ class Handle:
         rc = lib().zolo_set_option(self.ptr, option, value)
         if rc != 0:
             raise ZoloError(f"zolo_set_option({option}, {value})", rc)
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int()
+        rc = lib().zolo_get_option(self.ptr, option, C.byref(v))
+        if rc != 0:
+            raise ZoloError(f"zolo_get_option({option})", rc)
+        return v.value
 
     def profile(self, on: bool = True):
         lib().zolo_profile_enable(self.ptr, 1 if on else 0)

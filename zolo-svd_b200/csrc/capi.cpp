@@ -83,12 +83,84 @@ void qdwh_lwork(int m, int n, const int* desca, const int* descw, double* lwin, 
   *lwin2 = std::max(geqrf + 1.0, static_cast<double>(m) * n);
 }
 
-struct DevBuf {
-  double* p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
+struct DevView {
+  double* p;
 };
+
+// PZOLOPD1 semantics with ZOLO_OPT_OWN_BOUNDS: the caller's ALPHA and BETA are replaced by
+// the library's own (alpha = ||A||_F, beta from the QR of A/alpha) and that QR is reused by
+// the first iteration.  The polar factor does not depend on the scaling of A, so Q is the
+// same to rounding; SYM = 'S' keeps the caller's bounds.
+int zolo_pd_entry(Context& c, char sym, int rk, int m, int n, double alpha, double beta, const double* dA, int64_t lda,
+                  double* dQ, int64_t ldq, double* dH, int64_t ldh) {
+  if (c.zolo_own_bounds && !(sym == 'S' || sym == 's') && m >= n && rk >= 1 && rk <= 8)
+    return zolo::zolo_polar(c, rk, m, n, dA, lda, dQ, ldq, dH, ldh);
+  return zolo::zolo_pd(c, sym, rk, m, n, alpha, beta, dA, lda, dQ, ldq, dH, ldh);
+}
+
+// One algorithm option of a handle (zolo_set_option); 0, -1 unknown option, -3 bad value.
+int set_option(Context& c, int option, int value) {
+  switch (option) {
+    case ZOLO_OPT_SHARED_QR:
+      c.zolo_shared_qr = value != 0;
+      return 0;
+    case ZOLO_OPT_NS_FINISH:
+      c.zolo_ns_finish = value != 0;
+      return 0;
+    case ZOLO_OPT_CHOL_INVERSE:
+      c.zolo_chol_inverse = value != 0;
+      return 0;
+    case ZOLO_OPT_BETA_FROB:
+      c.zolo_beta_frob = value != 0;
+      return 0;
+    case ZOLO_OPT_TERM_PLAN:
+      c.zolo_term_plan = value != 0;
+      return 0;
+    case ZOLO_OPT_MIXED:
+      if (value < 0 || value > 1) return -3;
+      c.zolo_mixed = value;
+      return 0;
+    case ZOLO_OPT_MIXED_SLICES:
+      if (value < 6 || value > 8) return -3;
+      c.oz_slices = value;
+      return 0;
+    case ZOLO_OPT_OWN_BOUNDS:
+      c.zolo_own_bounds = value != 0;
+      return 0;
+    default:
+      return -1;
+  }
+}
+
+// Options of the default handle from the environment, so that callers of the reference's
+// entry points (pzolopd1_, pqdwhfacs_, ...) select them without a code change: ZOLO_FAST=1
+// turns on every cost option (shared QR, Newton-Schulz finish, explicit-inverse Cholesky,
+// Frobenius beta, term plan, own bounds); ZOLO_OPT_<NAME>=<value> sets one option and
+// overrides ZOLO_FAST.  Unparsable or out-of-range values are ignored.
+void apply_env_options(Context& c) {
+  auto get = [](const char* name, int* v) {
+    const char* s = std::getenv(name);
+    if (!s || !*s) return false;
+    char* end = nullptr;
+    const long x = std::strtol(s, &end, 10);
+    if (end == s || *end != '\0') return false;
+    *v = static_cast<int>(x);
+    return true;
+  };
+  int v = 0;
+  if (get("ZOLO_FAST", &v) && v) {
+    for (int o : {ZOLO_OPT_SHARED_QR, ZOLO_OPT_NS_FINISH, ZOLO_OPT_CHOL_INVERSE, ZOLO_OPT_BETA_FROB,
+                  ZOLO_OPT_TERM_PLAN, ZOLO_OPT_OWN_BOUNDS})
+      set_option(c, o, 1);
+  }
+  const std::pair<const char*, int> names[] = {
+      {"ZOLO_OPT_SHARED_QR", ZOLO_OPT_SHARED_QR},   {"ZOLO_OPT_NS_FINISH", ZOLO_OPT_NS_FINISH},
+      {"ZOLO_OPT_CHOL_INVERSE", ZOLO_OPT_CHOL_INVERSE}, {"ZOLO_OPT_BETA_FROB", ZOLO_OPT_BETA_FROB},
+      {"ZOLO_OPT_TERM_PLAN", ZOLO_OPT_TERM_PLAN},   {"ZOLO_OPT_MIXED", ZOLO_OPT_MIXED},
+      {"ZOLO_OPT_MIXED_SLICES", ZOLO_OPT_MIXED_SLICES}, {"ZOLO_OPT_OWN_BOUNDS", ZOLO_OPT_OWN_BOUNDS}};
+  for (const auto& nm : names)
+    if (get(nm.first, &v)) set_option(c, nm.second, v);
+}
 
 int run_qdwh_host(char sym, int m, int n, double sigma, const double* a, int ia, int ja, const int* desca, double* q,
                   int iq, int jq, const int* descq, double* work, int lwork, const int* descw, double* work2,
@@ -117,11 +189,10 @@ int run_qdwh_host(char sym, int m, int n, double sigma, const double* a, int ia,
   if (int e = zolo_default_handle(&h)) return e;
   const bool want_h = (polar == 'T' || polar == 't');
   return guarded(h, [&](Context& c) -> int {
-    DevBuf dA, dQ, dH;
+    // device copies of the caller's arrays: handle workspace, allocated once and reused
     const int64_t ld = m;
-    zolo::ck(cudaMalloc(&dA.p, sizeof(double) * m * n));
-    zolo::ck(cudaMalloc(&dQ.p, sizeof(double) * m * n));
-    if (want_h) zolo::ck(cudaMalloc(&dH.p, sizeof(double) * n * n));
+    const DevView dA{c.buf("host_a", static_cast<size_t>(m) * n)}, dQ{c.buf("host_q", static_cast<size_t>(m) * n)};
+    const DevView dH{want_h ? c.buf("host_h", static_cast<size_t>(n) * n) : nullptr};
     zolo::ck(cudaMemcpy2DAsync(dA.p, ld * sizeof(double), a, desca[8] * sizeof(double), m * sizeof(double), n,
                                cudaMemcpyHostToDevice, c.stream()));
     zolo::QdwhOpts o;
@@ -157,13 +228,12 @@ int run_zolo_host(char sym, int rk, int m, int n, double alpha, double beta, con
   zolo_handle_t h = nullptr;
   if (int e = zolo_default_handle(&h)) return e;
   return guarded(h, [&](Context& c) -> int {
-    DevBuf dA, dQ;
+    // device copies of the caller's arrays: handle workspace, allocated once and reused
     const int64_t ld = m;
-    zolo::ck(cudaMalloc(&dA.p, sizeof(double) * m * n));
-    zolo::ck(cudaMalloc(&dQ.p, sizeof(double) * m * n));
+    const DevView dA{c.buf("host_a", static_cast<size_t>(m) * n)}, dQ{c.buf("host_q", static_cast<size_t>(m) * n)};
     zolo::ck(cudaMemcpy2DAsync(dA.p, ld * sizeof(double), as, desca[8] * sizeof(double), m * sizeof(double), n,
                                cudaMemcpyHostToDevice, c.stream()));
-    const int info = zolo::zolo_pd(c, sym, rk, m, n, alpha, beta, dA.p, ld, dQ.p, ld, nullptr, 0);
+    const int info = zolo_pd_entry(c, sym, rk, m, n, alpha, beta, dA.p, ld, dQ.p, ld, nullptr, 0);
     zolo::ck(cudaMemcpy2DAsync(q, descq[8] * sizeof(double), dQ.p, ld * sizeof(double), m * sizeof(double), n,
                                cudaMemcpyDeviceToHost, c.stream()));
     zolo::ck(cudaStreamSynchronize(c.stream()));
@@ -207,6 +277,7 @@ int zolo_default_handle(zolo_handle_t* handle) {
     if (const char* s = std::getenv("ZOLO_DEVICE")) dev = std::atoi(s);
     const int e = zolo_create(dev, &g_default);
     if (e) return e;
+    apply_env_options(g_default->ctx);
   }
   *handle = g_default;
   return 0;
@@ -236,38 +307,23 @@ int zolo_profile_enable(zolo_handle_t h, int on) {
 }
 
 int zolo_set_option(zolo_handle_t h, int option, int value) {
+  return guarded(h, [&](Context& c) { return set_option(c, option, value); });
+}
+
+int zolo_get_option(zolo_handle_t h, int option, int* value) {
+  if (!value) return -3;
   return guarded(h, [&](Context& c) {
-    if (option == ZOLO_OPT_SHARED_QR) {
-      c.zolo_shared_qr = value != 0;
-      return 0;
+    switch (option) {
+      case ZOLO_OPT_SHARED_QR: *value = c.zolo_shared_qr; return 0;
+      case ZOLO_OPT_NS_FINISH: *value = c.zolo_ns_finish; return 0;
+      case ZOLO_OPT_CHOL_INVERSE: *value = c.zolo_chol_inverse; return 0;
+      case ZOLO_OPT_BETA_FROB: *value = c.zolo_beta_frob; return 0;
+      case ZOLO_OPT_TERM_PLAN: *value = c.zolo_term_plan; return 0;
+      case ZOLO_OPT_MIXED: *value = c.zolo_mixed; return 0;
+      case ZOLO_OPT_MIXED_SLICES: *value = c.oz_slices; return 0;
+      case ZOLO_OPT_OWN_BOUNDS: *value = c.zolo_own_bounds; return 0;
+      default: return -1;
     }
-    if (option == ZOLO_OPT_NS_FINISH) {
-      c.zolo_ns_finish = value != 0;
-      return 0;
-    }
-    if (option == ZOLO_OPT_CHOL_INVERSE) {
-      c.zolo_chol_inverse = value != 0;
-      return 0;
-    }
-    if (option == ZOLO_OPT_BETA_FROB) {
-      c.zolo_beta_frob = value != 0;
-      return 0;
-    }
-    if (option == ZOLO_OPT_TERM_PLAN) {
-      c.zolo_term_plan = value != 0;
-      return 0;
-    }
-    if (option == ZOLO_OPT_MIXED) {
-      if (value < 0 || value > 1) return -3;
-      c.zolo_mixed = value;
-      return 0;
-    }
-    if (option == ZOLO_OPT_MIXED_SLICES) {
-      if (value < 6 || value > 8) return -3;
-      c.oz_slices = value;
-      return 0;
-    }
-    return -1;
   });
 }
 
@@ -433,7 +489,7 @@ int zolo_polar_dev(zolo_handle_t h, int rk, int m, int n, const double* dA, int6
 int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double alpha, double beta, const double* dA,
                       int64_t lda, double* dQ, int64_t ldq, double* dH, int64_t ldh) {
   return guarded(h, [&](Context& c) {
-    return zolo::zolo_pd(c, sym, rk, m, n, alpha, beta, dA, lda, dQ, ldq, dH, ldh);
+    return zolo_pd_entry(c, sym, rk, m, n, alpha, beta, dA, lda, dQ, ldq, dH, ldh);
   });
 }
 
@@ -497,14 +553,10 @@ void zolo_zoloeig(int n, int /*nblk*/, double* q, double* as, int /*contxt*/, in
     r = zolo_default_handle(&h);
     if (r == 0)
       r = guarded(h, [&](Context& c) -> int {
-        DevBuf dQ, dA, dV, dE, dW, dZ;
+        // device copies of the caller's arrays: handle workspace, allocated once and reused
         const size_t nn = static_cast<size_t>(n) * n;
-        zolo::ck(cudaMalloc(&dQ.p, nn * 8));
-        zolo::ck(cudaMalloc(&dA.p, nn * 8));
-        zolo::ck(cudaMalloc(&dV.p, nn * 8));
-        zolo::ck(cudaMalloc(&dE.p, nn * 8));
-        zolo::ck(cudaMalloc(&dW.p, static_cast<size_t>(n) * 8));
-        zolo::ck(cudaMalloc(&dZ.p, nn * 8));
+        const DevView dQ{c.buf("host_q", nn)}, dA{c.buf("host_a", nn)}, dV{c.buf("host_v", nn)};
+        const DevView dE{c.buf("host_e", nn)}, dW{c.buf("host_w", n)}, dZ{c.buf("host_z", nn)};
         zolo::ck(cudaMemcpyAsync(dQ.p, q, nn * 8, cudaMemcpyHostToDevice, c.stream()));
         zolo::ck(cudaMemcpyAsync(dA.p, as, nn * 8, cudaMemcpyHostToDevice, c.stream()));
         int rk = 0;

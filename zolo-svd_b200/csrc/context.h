@@ -104,6 +104,8 @@ class Context {
   // Cholesky iterations, the Newton-Schulz finish and Q, H run on the INT8-emulated GEMM
   // (ozgemm, oz_slices digit planes); the bounds and the QR iterations stay on DMMA.
   int zolo_mixed = 0;
+  // PZOLOPD1 entries: 1 = compute ALPHA, BETA from A (zolo_polar) instead of the caller's
+  int zolo_own_bounds = 0;
   int oz_slices = 8;
   // digit planes of the products gemm() routes to ozgemm right now (0 = none); set by OzScope
   int oz_active = 0;
