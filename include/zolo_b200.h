@@ -189,7 +189,7 @@ void zolo_mellipke(double alpha, double tol, double* k, double* e);
 void zolo_mellipj(double u, double alpha, double tol, double* sn, double* cn, double* dn);
 /* choosem (Auxil_Zolo.f90:130-163) */
 int zolo_choosem(double con);
-/* hfunc (hfunc.f90:204-244) */
+/* hfunc (hfunc.f90:2-42) */
 double zolo_hfunc(double x);
 /* FONE and next CON of a Zolo iteration (pzolopd1.f90:459-472) */
 void zolo_fone_next(double con, const double* coeff, int rk, double* fone, double* next_con);

@@ -163,7 +163,7 @@ def zolo_next_con(con: float, coeff: np.ndarray, rk: int, fone: float) -> float:
 
 
 def hfunc(x: float) -> float:
-    """QDWH dynamical weight a(l) (hfunc.f90:204-244)."""
+    """QDWH dynamical weight a(l) (hfunc.f90:2-42; the formula at 26-39)."""
     tol = 30.0 * EPS
     x2 = x * x
     if abs(x - 1.0) <= tol:
@@ -217,8 +217,8 @@ def bounds_pqdwhfacs(x0: np.ndarray) -> tuple[float, int]:
 def bounds_qr_condest(x0: np.ndarray) -> tuple[float, int]:
     """sigma_min lower-bound estimate from R of X0 = QR: 1/(sqrt(n) * ||R^-1||_1).
 
-    ||R^-1||_1 is evaluated exactly here (dtrtri), which the GPU's Hager-Higham
-    estimator approximates from below.
+    ||R^-1||_1 is evaluated exactly here (dtrtri), as on the GPU, which forms R^-1
+    with its blocked triangular inverse and takes its exact norm.
     """
     n = x0.shape[1]
     r = np.triu(sla.qr(x0, mode="r")[0][:n, :n])

@@ -5,7 +5,7 @@
 1. ``zolo_scalars.json``: Zolotarev shifts c_i, weights a_i, FONE and the next
    CON for (CON, r) pairs, and the QDWH weight h(l), all evaluated with mpmath
    at 50 digits -- independently of the double-precision AGM / Landen code the
-   reference uses (Auxil_Zolo.f90:36-200, hfunc.f90:204-244).  The modulus is
+   reference uses (Auxil_Zolo.f90:36-200, hfunc.f90:2-42).  The modulus is
    taken from the double value alpha = acos(1/CON) exactly as the reference
    forms it (Auxil_Zolo.f90:176-177), so the fixture pins the elliptic-function
    evaluation, not the rounding of alpha.

@@ -1,6 +1,6 @@
 // Host scalar code of the polar iterations: Zolotarev coefficients
 // (Auxil_Zolo.f90:36-200), the Zolo FONE / CON recursion (pzolopd1.f90:459-472)
-// and the QDWH dynamical weights (hfunc.f90:204-244, pqdwhfacs.f90:361-368).
+// and the QDWH dynamical weights (hfunc.f90:2-42, pqdwhfacs.f90:361-368).
 // Written in double precision with the same operation order as the reference
 // so that the iteration control (branch choice, stopping test) matches it.
 #include "coeff.h"
