@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--n", "--matrix-n", dest="n", type=int, default=8192)
     ap.add_argument("--rk", type=int, default=8)
     ap.add_argument("--kappa", type=float, default=1e12)
-    ap.add_argument("--ref-timeout", type=float, default=1500.0,
+    ap.add_argument("--ref-timeout", type=float, default=1650.0,
                     help="seconds allowed for the reference arm's one full CPU solve")
     return ap.parse_args()
 
@@ -168,28 +168,48 @@ def fp64_peak_tflops(torch) -> float:
 # ---------------------------------------------------------------------------
 # CPU reference arm: the oracle restatement, one full solve of the same matrix
 # ---------------------------------------------------------------------------
-def _oracle_solve(n: int, rk: int, kappa: float, seed: int, conn) -> None:
+def _oracle_solve(n: int, rk: int, kappa: float, seed: int, groups: int, conn) -> None:
     """Child process: generate the matrix, run bounds + PZOLOPD1 + H of the oracle, send the
-    timings (the generation is outside the timed region)."""
+    timings (the generation is outside the timed region).  With groups > 1 the r terms of each
+    iteration run on `groups` worker processes of cores/groups BLAS threads each, as the
+    reference runs them on r MPI process groups (pzolopd1.f90:298-374)."""
     sys.path.insert(0, ROOT)
     from oracle import zolo_oracle as zo  # the CPU restatement, used only as the baseline
     a, _ = make_input(n, kappa, seed)
+    pool = None
+    term_map = None
+    if groups > 1:
+        import multiprocessing as mp
+        threads = max(1, (os.cpu_count() or 1) // groups)
+        saved = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS")}
+        os.environ["OPENBLAS_NUM_THREADS"] = os.environ["OMP_NUM_THREADS"] = str(threads)
+        pool = mp.get_context("spawn").Pool(groups)
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+        pool.starmap(zo.hfunc, [(0.5,)] * groups)  # workers started and the oracle imported
+        term_map = lambda fn, args: pool.starmap(fn, args)
     t0 = time.perf_counter()
     al, be, _ = zo.bounds_zolodrv(a)
-    q, st = zo.pzolopd1("N", rk, a, al, be)
+    q, st = zo.pzolopd1("N", rk, a, al, be, term_map=term_map)
     h = zo.polar_h(q, a)
     t = time.perf_counter() - t0
+    if pool:
+        pool.close()
+        pool.join()
     conn.send({"seconds": t, "iterations": st.iterations, "branches": st.branches,
                "backward_error": zo.backward_error(a, q, h), "orthogonality": zo.orthogonality(q)})
     conn.close()
 
 
-def oracle_full_solve(n: int, rk: int, kappa: float, seed: int, timeout: float) -> dict:
+def oracle_full_solve(n: int, rk: int, kappa: float, seed: int, timeout: float, groups: int = 1) -> dict:
     """One timed oracle solve in a spawned process (killed after `timeout` s)."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     parent, child = ctx.Pipe(duplex=False)
-    p = ctx.Process(target=_oracle_solve, args=(n, rk, kappa, seed, child))
+    p = ctx.Process(target=_oracle_solve, args=(n, rk, kappa, seed, groups, child))
     p.start()
     child.close()
     out = None
@@ -206,10 +226,13 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cores = os.cpu_count()
-    res = oracle_full_solve(args.n, args.rk, args.kappa, 1003, args.ref_timeout)
-    sample = (f"oracle bounds + pzolopd1 + H (NumPy/OpenBLAS, {cores} threads, 1x1 grid, no MPI) on the bench's "
-              f"own n={args.n}, kappa={args.kappa:g} matrix (PCG64 seed 1003): one full solve, no scaling")
+    cores = os.cpu_count() or 1
+    groups = max(1, min(args.rk, cores // 2))
+    res = oracle_full_solve(args.n, args.rk, args.kappa, 1003, args.ref_timeout, groups)
+    sample = (f"oracle bounds + pzolopd1 + H (NumPy/OpenBLAS) on the bench's own n={args.n}, "
+              f"kappa={args.kappa:g} matrix (PCG64 seed 1003): one full solve, no scaling; the r terms of each "
+              f"iteration on {groups} worker processes x {max(1, cores // groups)} BLAS threads (the reference's "
+              f"r process groups), bounds and H on {cores} threads; {cores} host cores")
     v = res["seconds"] if res else None
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": 1 if res else 0, "steps_requested": args.steps, "warmup": 0,

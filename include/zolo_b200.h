@@ -157,6 +157,12 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * on the scaling of A, so Q is the same to rounding; SYM = 'S' keeps the caller's values.
  * The caller still passes ALPHA, BETA > 0 (checked as before).  No reference counterpart. */
 #define ZOLO_OPT_OWN_BOUNDS 8
+/* ZOLO_OPT_INJECT_CHOL_FAIL (diagnostic, 0 = off): k + 1 makes the Cholesky-form step of
+ * iteration k report a failed factorization (INFO = 1000000 in zolo_stats_t.info) so that
+ * the recovery path runs: the step is redone in the QR form, as for a shifted Gram that is
+ * not numerically positive definite (the reference ignores PDPOSV's INFO).  Host-side only:
+ * no kernel is made to fail. */
+#define ZOLO_OPT_INJECT_CHOL_FAIL 9
 /* The default handle (used by the reference-named host-array entry points) reads its options
  * from the environment when it is created, so an unchanged Fortran driver selects them:
  * ZOLO_FAST=1 sets ZOLO_OPT_SHARED_QR, _NS_FINISH, _CHOL_INVERSE, _BETA_FROB, _TERM_PLAN and
@@ -261,6 +267,22 @@ int zolo_qdwh_dev(zolo_handle_t h, char sym, int m, int n, double sigma, const d
 int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, const double* const* dA,
                         const int64_t* lda, double* const* dQ, const int64_t* ldq, double* const* dH,
                         const int64_t* ldh, int* info, int* iterations);
+/* Bucket plan of zolo_qdwh_batch_dev (no reference counterpart).  The members, sorted by n,
+ * are split into contiguous runs; each run is one batched solve padded to NB = its largest n
+ * and MB = its largest m + NB - n (multiples of 32), and the runs execute concurrently on
+ * model[4] worker streams.  The split minimizes the predicted time of the cost model
+ *   ms(bucket) = model[0] + model[1] * NB/32 + B * flops(MB, NB) / (model[2] TFLOP/s * NB/(NB + model[3]))
+ * (launch-chain latency, shared by the worker streams, plus the members' padded work) by
+ * dynamic programming.  zolo_batch_autotune measures the model on the handle's GPU (probe
+ * buckets of 1 and 8 members at n = 64, 256, 1024) and stores it in the handle;
+ * zolo_batch_set_model sets it (5 values).  zolo_batch_plan (host only, no GPU) returns the
+ * number of buckets and fills bucket[i] (member i's bucket), mb[], nb[] (per bucket, count
+ * entries suffice) and the predicted ms; model NULL = the defaults; mode 1 = the fixed size
+ * ladder instead of the optimized split. */
+int zolo_batch_autotune(zolo_handle_t h, double* model);
+int zolo_batch_set_model(zolo_handle_t h, const double* model);
+int zolo_batch_plan(int count, const int* m, const int* n, const double* model, int max_batch, int mode,
+                    int* bucket, int* mb, int* nb, double* predicted_ms);
 /* The reference driver's sequence in one call (test_zolodrv1.f90:167-198: the bounds,
  * then PZOLOPD1 with SYM = 'N'), plus H when dH is not NULL: alpha = ||A||_F and
  * beta = 1/(sqrt(n) ||R^{-1}||_1) as zolo_bounds_dev mode 1, then Zolo-PD with rk

@@ -309,9 +309,21 @@ class PDStats:
     info: int = 0
 
 
+def zolo_term(kind: str, sym: str, x: np.ndarray, coeff: np.ndarray, rk: int, ip: int) -> tuple[np.ndarray, int]:
+    """Term ip of one Zolo-PD iteration: ZOLOQR (kind 'QR') or ZOLOCHOL (kind 'CH'), with INFO."""
+    if kind == "QR":
+        return zoloqr(x, coeff, rk, ip), 0
+    return zolochol(sym, x, coeff, rk, ip)
+
+
 def pzolopd1(sym: str, rk: int, a: np.ndarray, alpha: float, beta: float,
-             maxit: int = 6) -> tuple[np.ndarray, PDStats]:
-    """Zolo-PD with the r terms run one after another (pzolopd1.f90:280-487)."""
+             maxit: int = 6, term_map=None) -> tuple[np.ndarray, PDStats]:
+    """Zolo-PD (pzolopd1.f90:280-487).  The r terms of an iteration are evaluated by
+    ``term_map(zolo_term, [(kind, sym, x, coeff, rk, ip), ...])`` -- serially by default; a
+    process pool gives the reference's r concurrent process groups (pzolopd1.f90:298-374) --
+    and summed in term order (the DGSUM2D of pzolopd1.f90:424-429, 447-451)."""
+    if term_map is None:
+        term_map = lambda fn, args: [fn(*x) for x in args]
     st = PDStats(alpha=alpha, beta=beta)
     scale = alpha * beta
     con = 1.0 / beta
@@ -326,17 +338,12 @@ def pzolopd1(sym: str, rk: int, a: np.ndarray, alpha: float, beta: float,
         coeff = compute_coeff(con, tol, rk)
         maxc = float(np.max(coeff[: 2 * rk]))
         z = np.zeros_like(x)
-        if (it == 0 or con > 1.0e3) and maxc > 3.0e2:
-            st.branches.append("QR")
-            for ip in range(1, rk + 1):
-                z += zoloqr(x, coeff, rk, ip)
-        else:
-            st.branches.append("CH")
-            for ip in range(1, rk + 1):
-                zt, info = zolochol(sym, x, coeff, rk, ip)
-                if info != 0 and st.info == 0:
-                    st.info = info
-                z += zt
+        kind = "QR" if (it == 0 or con > 1.0e3) and maxc > 3.0e2 else "CH"
+        st.branches.append(kind)
+        for zt, info in term_map(zolo_term, [(kind, sym, x, coeff, rk, ip) for ip in range(1, rk + 1)]):
+            if info != 0 and st.info == 0:
+                st.info = info
+            z += zt
         st.con.append(con)
         fone = zolo_fone(coeff, rk)
         con = zolo_next_con(con, coeff, rk, fone)

@@ -86,3 +86,52 @@ def test_batch_bad_member_and_empty():
         assert zo.orthogonality(q) <= tol_n(a.shape[1])
     assert zb.qdwh_batch_dev(h, []) == ([], [])
     h.close()
+
+
+def config4_members(seed=1004, count=512):
+    """Configuration 4: n = round(exp U[ln 64, ln 1024]), m = round(n (1 + U[0, 1])),
+    kappa = 10^U[2, 14], s geometric from 1 to 1/kappa; member i generated from PCG64 seed
+    seed + i (Haar U m x n, V n x n)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        m = int(round(n * (1 + rng.uniform(0, 1))))
+        kappa = 10 ** rng.uniform(2, 14)
+        s = np.geomspace(1.0, 1.0 / kappa, n)
+        a, u, v = zo.make_matrix(n, s, seed + i, m=m)
+        out.append((a, u, v, s, kappa))
+    return out
+
+
+def test_batch_config4_full_size():
+    """The 512-member configuration at full size in one call: every member backward stable and
+    orthogonal to 10 n eps, its singular values within 1e-12 sigma_max, its polar factor within
+    100 n eps kappa of U V^T; a sample of members against the oracle's PQDWHFACS."""
+    import torch
+    h = zb.Handle(0)
+    mats = config4_members()
+    dev = [zb.colmajor_to_device(a) for a, *_ in mats]
+    dq = [torch.zeros_like(d) for d in dev]
+    dh = [torch.zeros((a.shape[1], a.shape[1]), dtype=torch.float64, device="cuda") for a, *_ in mats]
+    torch.cuda.synchronize()
+    members = [(a.shape[0], a.shape[1], d.data_ptr(), a.shape[0], q.data_ptr(), a.shape[0], hh.data_ptr(),
+                a.shape[1]) for (a, *_), d, q, hh in zip(mats, dev, dq, dh)]
+    info, its = zb.qdwh_batch_dev(h, members)
+    assert info == [0] * len(mats)
+    worst = 0.0
+    for k, ((a, u, v, s, kappa), q_d, h_d) in enumerate(zip(mats, dq, dh)):
+        m, n = a.shape
+        q, hh = zb.device_to_colmajor(q_d), zb.device_to_colmajor(h_d)
+        be, orth = zo.backward_error(a, q, hh), zo.orthogonality(q)
+        worst = max(worst, be / (10 * n * EPS), orth / (10 * n * EPS))
+        assert be <= tol_n(n) and orth <= tol_n(n), (k, be, orth)
+        ev = np.sort(np.linalg.eigvalsh(0.5 * (hh + hh.T)))[::-1]
+        assert np.max(np.abs(ev - s)) <= 1e-12 * s[0], k
+        assert np.linalg.norm(q - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa), k
+        if k % 64 == 0:  # a sample against the oracle on the same member
+            q_o, h_o, st_o = zo.pqdwhfacs("N", a, bounds="qr")
+            assert np.linalg.norm(q - q_o) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa), k
+            assert abs(its[k] - st_o.iterations) <= 2, (k, its[k], st_o.iterations)  # padding shifts beta
+    assert worst <= 1.0
+    h.close()

@@ -475,3 +475,44 @@ def test_fast_form_small_sizes(m, n):
     check_pd(a, q, hh, n)
     np.testing.assert_array_equal(q, q2)
     assert np.linalg.norm(q - u @ v.T) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * 1e6)
+
+
+def _run_polar(h, a, m, n, fast, inject=0, qdwh=False):
+    import torch
+    da = zb.colmajor_to_device(a)
+    dq = torch.zeros_like(da)
+    dh = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    for opt in (zb.OPT_SHARED_QR, zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_BETA_FROB, zb.OPT_TERM_PLAN):
+        h.set_option(opt, 1 if fast else (1 if opt == zb.OPT_SHARED_QR else 0))
+    h.set_option(zb.OPT_INJECT_CHOL_FAIL, inject)
+    torch.cuda.synchronize()
+    if qdwh:
+        info = zb.qdwh_dev(h, "N", m, n, 0.0, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n, 0, 12, 0)
+    elif fast:
+        info = zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n)
+    else:
+        al, be, _ = zo.bounds_zolodrv(a)
+        info = zb.pzolopd1_dev(h, "N", 8, m, n, al, be, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n)
+    h.set_option(zb.OPT_INJECT_CHOL_FAIL, 0)
+    return info, zb.device_to_colmajor(dq), zb.device_to_colmajor(dh), h.stats()
+
+
+@pytest.mark.parametrize("path", ["zolo_fast", "zolo_reference_rule", "qdwh"])
+def test_cholesky_failure_recovers_with_qr_form(path):
+    """A Cholesky-form step whose shifted Gram is reported not positive definite (host-side
+    injection, ZOLO_OPT_INJECT_CHOL_FAIL) is redone in the QR form: INFO recorded in the stats,
+    that iteration's branch is QR, and the result keeps the 10 n eps accuracy."""
+    m, n, kappa = 300, 260, 1e8
+    a, u, v = zo.make_matrix(n, np.geomspace(1.0, 1.0 / kappa, n), 910, m=m)
+    h = zb.Handle(0)
+    fast, qdwh = path == "zolo_fast", path == "qdwh"
+    info0, q0, h0, st0 = _run_polar(h, a, m, n, fast, 0, qdwh)
+    assert info0 == 0 and st0["info"] == 0
+    k = st0["branches"].index("CH")  # first Cholesky-form iteration
+    info1, q1, h1, st1 = _run_polar(h, a, m, n, fast, k + 1, qdwh)
+    h.close()
+    assert info1 == 0  # the solve completes; the factorization failure is reported in the stats
+    assert st1["info"] == 1000000
+    assert st1["branches"][k] == "QR" and st1["branches"][:k] == st0["branches"][:k]
+    check_pd(a, q1, h1, n)
+    assert np.linalg.norm(q1 - q0) / math.sqrt(n) <= 100 * n * EPS * kappa

@@ -121,6 +121,10 @@ _SIGS = [
     ("zolo_ozgemm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double,
                                   C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_int64,
                                   C.c_int, C.c_int, C.c_int]),
+    ("zolo_batch_autotune", C.c_int, [C.c_void_p, c_double_p]),
+    ("zolo_batch_set_model", C.c_int, [C.c_void_p, c_double_p]),
+    ("zolo_batch_plan", C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p,
+                                  c_int_p, c_double_p]),
     ("zolo_dpotrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
     ("zolo_dtrsm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                  C.c_int64, C.c_void_p, C.c_int64]),
@@ -153,6 +157,7 @@ OPT_TERM_PLAN = 5
 OPT_MIXED = 6
 OPT_MIXED_SLICES = 7
 OPT_OWN_BOUNDS = 8
+OPT_INJECT_CHOL_FAIL = 9
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
                    "ozgemm"]
 
@@ -309,6 +314,25 @@ def pzolopd1(sym: str, rk: int, a: np.ndarray, alpha: float, beta: float, polar:
     lib().zolo_pzolopd1(sym.encode()[:1], rk, m, n, alpha, beta, _dp(a), 1, 1, d.ctypes.data_as(c_int_p), _dp(q),
                         1, 1, d.ctypes.data_as(c_int_p), C.byref(info), polar.encode()[:1])
     return q, info.value
+
+
+def batch_plan(m, n, model=None, max_batch: int = 1024, mode: int = 0):
+    """The bucket plan of the batched solver (host only): (bucket of each member, [(MB, NB)]
+    per bucket, predicted ms).  mode 1 = the fixed size ladder."""
+    m = np.ascontiguousarray(m, dtype=np.int32)
+    n = np.ascontiguousarray(n, dtype=np.int32)
+    k = len(n)
+    bucket = np.zeros(k, dtype=np.int32)
+    mb = np.zeros(max(k, 1), dtype=np.int32)
+    nb = np.zeros(max(k, 1), dtype=np.int32)
+    pred = C.c_double()
+    mdl = None if model is None else np.ascontiguousarray(model, dtype=np.float64)
+    r = lib().zolo_batch_plan(k, m.ctypes.data_as(c_int_p), n.ctypes.data_as(c_int_p),
+                              None if mdl is None else _dp(mdl), max_batch, mode, bucket.ctypes.data_as(c_int_p),
+                              mb.ctypes.data_as(c_int_p), nb.ctypes.data_as(c_int_p), C.byref(pred))
+    if r < 0:
+        raise ZoloError("zolo_batch_plan", r)
+    return bucket, [(int(mb[b]), int(nb[b])) for b in range(r)], pred.value
 
 
 def pzolopd_f77(sym: str, rk: int, m: int, n: int, alpha: float, beta: float, a_ptr: int, lda: int, q_ptr: int,

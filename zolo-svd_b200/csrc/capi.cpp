@@ -127,6 +127,10 @@ int set_option(Context& c, int option, int value) {
     case ZOLO_OPT_OWN_BOUNDS:
       c.zolo_own_bounds = value != 0;
       return 0;
+    case ZOLO_OPT_INJECT_CHOL_FAIL:
+      if (value < 0) return -3;
+      c.inject_chol_fail = value;
+      return 0;
     default:
       return -1;
   }
@@ -322,6 +326,7 @@ int zolo_get_option(zolo_handle_t h, int option, int* value) {
       case ZOLO_OPT_MIXED: *value = c.zolo_mixed; return 0;
       case ZOLO_OPT_MIXED_SLICES: *value = c.oz_slices; return 0;
       case ZOLO_OPT_OWN_BOUNDS: *value = c.zolo_own_bounds; return 0;
+      case ZOLO_OPT_INJECT_CHOL_FAIL: *value = c.inject_chol_fail; return 0;
       default: return -1;
     }
   });
@@ -477,6 +482,52 @@ int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, 
   return guarded(h, [&](Context& c) {
     return zolo::qdwh_batch(c, count, m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, nullptr);
   });
+}
+
+int zolo_batch_autotune(zolo_handle_t h, double* model) {
+  return guarded(h, [&](Context& c) {
+    zolo::batch_autotune(c);
+    if (model) {
+      const zolo::BatchCostModel& md = c.batch_model;
+      model[0] = md.lat0;
+      model[1] = md.lat1;
+      model[2] = md.rate_tflops;
+      model[3] = md.nhalf;
+      model[4] = md.streams;
+    }
+    return 0;
+  });
+}
+
+int zolo_batch_set_model(zolo_handle_t h, const double* model) {
+  if (!model) return -2;
+  if (!(model[0] >= 0.0) || !(model[1] >= 0.0) || !(model[2] > 0.0) || !(model[3] >= 0.0) || !(model[4] >= 1.0) ||
+      model[4] > 16.0)
+    return -2;
+  return guarded(h, [&](Context& c) {
+    c.batch_model = zolo::BatchCostModel{model[0], model[1], model[2], model[3], static_cast<int>(model[4])};
+    return 0;
+  });
+}
+
+int zolo_batch_plan(int count, const int* m, const int* n, const double* model, int max_batch, int mode,
+                    int* bucket, int* mb, int* nb, double* predicted_ms) {
+  if (count < 0) return -1;
+  if (count > 0 && (!m || !n || !bucket || !mb || !nb)) return -2;
+  if (max_batch < 1) return -5;
+  for (int i = 0; i < count; ++i)
+    if (n[i] < 1 || m[i] < n[i]) return -3;
+  zolo::BatchCostModel md;
+  if (model) md = zolo::BatchCostModel{model[0], model[1], model[2], model[3], static_cast<int>(model[4])};
+  const zolo::BucketPlan p = mode == 1 ? zolo::ladder_buckets(md, count, m, n, max_batch)
+                                       : zolo::plan_buckets(md, count, m, n, max_batch);
+  for (size_t b = 0; b < p.members.size(); ++b) {
+    for (int i : p.members[b]) bucket[i] = static_cast<int>(b);
+    mb[b] = p.mb[b];
+    nb[b] = p.nb[b];
+  }
+  if (predicted_ms) *predicted_ms = p.total_ms;
+  return static_cast<int>(p.members.size());
 }
 
 int zolo_polar_dev(zolo_handle_t h, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq,

@@ -25,6 +25,7 @@ Context::~Context() {
 }
 
 void Context::release_all() {
+  workers.clear();
   if (stream_) cudaStreamSynchronize(stream_);
   if (side_) cudaStreamSynchronize(side_);
   for (auto& kv : bufs_) cudaFree(kv.second.first);

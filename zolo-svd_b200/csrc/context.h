@@ -8,6 +8,9 @@
 #include <string>
 #include <vector>
 
+#include <memory>
+
+#include "batch_plan.h"
 #include "kernels.h"
 
 namespace zolo {
@@ -106,6 +109,12 @@ class Context {
   int zolo_mixed = 0;
   // PZOLOPD1 entries: 1 = compute ALPHA, BETA from A (zolo_polar) instead of the caller's
   int zolo_own_bounds = 0;
+  // diagnostic: k + 1 = the Cholesky step of iteration k reports failure (0 = off)
+  int inject_chol_fail = 0;
+  // batched solver: cost model of its bucket plan, and the worker contexts (own stream and
+  // workspace each) its buckets run on concurrently
+  BatchCostModel batch_model;
+  std::vector<std::unique_ptr<Context>> workers;
   int oz_slices = 8;
   // digit planes of the products gemm() routes to ozgemm right now (0 = none); set by OzScope
   int oz_active = 0;

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <thread>
 #include <vector>
 
 #include "coeff.h"
@@ -62,6 +63,13 @@ struct EventTimer {
 };
 
 int npanels(int n) { return (n + 31) / 32; }
+
+// Host-side fault injection (ZOLO_OPT_INJECT_CHOL_FAIL = k + 1): the Cholesky-form step of
+// iteration k reports a failed factorization (INFO = n + 1, beyond any real pivot index)
+// and takes the recovery path, as a non-positive-definite shifted Gram would.
+int injected_info(const Context& c, int it, int info) {
+  return (c.inject_chol_fail == it + 1 && info == 0) ? 1000000 : info;
+}
 
 // With the mixed form on: 0, or -2000 - code when a pipeline wait of an INT8-emulated product
 // timed out during the solve (its results are then not to be used).
@@ -423,7 +431,7 @@ int qdwh(Context& c, int m, int n, const double* dA, int64_t lda, double* dQ, in
       ck(cudaMemsetAsync(dinfo, 0, sizeof(int), c.stream()));
       c.stats.launches += 2;
       potrf(c, n, G, 1, dinfo, Dg);
-      const int pinfo = read_info(c, dinfo, 1);
+      const int pinfo = injected_info(c, it, read_info(c, dinfo, 1));
       if (pinfo != 0) {
         // not numerically SPD: redo this step with the QR form (the reference ignores PDPOSV's INFO)
         if (c.stats.info == 0) c.stats.info = pinfo;
@@ -586,7 +594,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       } else {
         potrf(c, n, Wc, rk_it, dinfo, Dz);
       }
-      const int pinfo = read_info(c, dinfo, rk_it);
+      const int pinfo = injected_info(c, it, read_info(c, dinfo, rk_it));
       if (pinfo != 0) {
         if (c.stats.info == 0) c.stats.info = pinfo;
         use_qr = true;  // fall back to the QR form for this step
@@ -752,15 +760,6 @@ int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, 
 }
 
 namespace {
-
-// padded sizes of the batch buckets: multiples of 32 about 1.2x apart
-int bucket_size(int n) {
-  static const int ladder[] = {32,  64,  96,  128, 160, 192,  224,  256,  320,  384,  448,  512,
-                               640, 768, 896, 1024, 1280, 1536, 1792, 2048, 2560, 3072, 3584, 4096};
-  for (int v : ladder)
-    if (n <= v) return v;
-  return (n + 511) / 512 * 512;
-}
 
 constexpr int kMaxBatch = 1024;  // members per launch (the device INFO array holds 1024)
 
@@ -995,24 +994,143 @@ int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* 
   *bs = BatchStats{};
   c.stats = Stats{};
   EventTimer total(c.stream());
-  std::map<int, std::vector<int>> buckets;
-  for (int i = 0; i < count; ++i) buckets[bucket_size(n[i])].push_back(i);
-  for (const auto& kv : buckets) {
-    const int NB = kv.first;
-    const std::vector<int>& all = kv.second;
-    for (size_t off = 0; off < all.size(); off += kMaxBatch) {
-      const std::vector<int> idx(all.begin() + off, all.begin() + std::min(all.size(), off + kMaxBatch));
-      int MB = NB;
-      for (int i : idx) MB = std::max(MB, m[i] + NB - n[i]);
-      MB = (MB + 31) / 32 * 32;
-      qdwh_bucket(c, idx, MB, NB, m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, bs);
+  // buckets from the cost model (dynamic programming over the members sorted by n)
+  const BucketPlan plan = plan_buckets(c.batch_model, count, m, n, kMaxBatch);
+  const int nbk = static_cast<int>(plan.nb.size());
+  const int W = std::min(std::max(1, c.batch_model.streams), nbk);
+  if (W <= 1) {
+    for (int b = 0; b < nbk; ++b)
+      qdwh_bucket(c, plan.members[b], plan.mb[b], plan.nb[b], m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, bs);
+  } else {
+    // the buckets are independent: spread them over W worker contexts (own stream and
+    // workspace each, driven by one host thread each) so that their launch chains overlap
+    while (static_cast<int>(c.workers.size()) < W) c.workers.emplace_back(new Context(c.device()));
+    std::vector<int> order(nbk);
+    for (int b = 0; b < nbk; ++b) order[b] = b;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return plan.ms[a] > plan.ms[b]; });
+    std::vector<std::vector<int>> assign(W);
+    std::vector<double> load(W, 0.0);
+    for (int b : order) {
+      const int w = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      assign[w].push_back(b);
+      load[w] += plan.ms[b];
+    }
+    // the members' inputs are ready on the caller's stream; the outputs are ready for it after
+    cudaEvent_t ready = c.event(0);
+    ck(cudaEventRecord(ready, c.stream()));
+    std::vector<BatchStats> wbs(W);
+    std::vector<int64_t> wl(W, 0);
+    std::vector<cudaError_t> werr(W, cudaSuccess);
+    std::vector<std::thread> th;
+    for (int w = 0; w < W; ++w) {
+      th.emplace_back([&, w] {
+        try {
+          Context& wc = *c.workers[w];
+          ck(cudaSetDevice(wc.device()));
+          ck(cudaStreamWaitEvent(wc.stream(), ready, 0));
+          wc.stats = Stats{};
+          for (int b : assign[w])
+            qdwh_bucket(wc, plan.members[b], plan.mb[b], plan.nb[b], m, n, dA, lda, dQ, ldq, dH, ldh, info,
+                        iterations, &wbs[w]);
+          wl[w] = wc.stats.launches;
+        } catch (const CudaFailure& e) {
+          werr[w] = e.err;
+        } catch (...) {
+          werr[w] = cudaErrorUnknown;
+        }
+      });
+    }
+    for (auto& t : th) t.join();
+    for (int w = 0; w < W; ++w) {
+      Context& wc = *c.workers[w];
+      ck(cudaEventRecord(wc.event(0), wc.stream()));
+      ck(cudaStreamWaitEvent(c.stream(), wc.event(0), 0));
+    }
+    for (int w = 0; w < W; ++w)
+      if (werr[w] != cudaSuccess) throw CudaFailure{werr[w]};
+    for (int w = 0; w < W; ++w) {
+      bs->buckets += wbs[w].buckets;
+      bs->max_iterations = std::max(bs->max_iterations, wbs[w].max_iterations);
+      bs->flops += wbs[w].flops;
+      bs->flops_useful += wbs[w].flops_useful;
+      c.stats.launches += wl[w];
     }
   }
   bs->ms = total.stop();
+  bs->predicted_ms = plan.total_ms;
   c.stats.ms_total = bs->ms;
   c.stats.flops = bs->flops_useful;
   c.stats.flops_exec_delta = bs->flops - bs->flops_useful;
   c.stats.iterations = bs->max_iterations;
+  return 0;
+}
+
+int batch_autotune(Context& c) {
+  // probe buckets of graded diagonal members (kappa 1e8, m = 1.5 n) at three sizes with 1 and
+  // 8 members: the difference gives the per-member work, the rest the launch-chain latency
+  const int sizes[3] = {64, 256, 1024};
+  double lat[3], rate[3];
+  double flops_at[3];
+  for (int k = 0; k < 3; ++k) {
+    const int NB = sizes[k], MB = NB + NB / 2;
+    std::vector<double> host(static_cast<size_t>(MB) * NB, 0.0);
+    for (int j = 0; j < NB; ++j) host[j + static_cast<size_t>(j) * MB] = std::pow(10.0, -8.0 * j / std::max(1, NB - 1));
+    const int B = 8;
+    double* dA = c.buf("tune_a", static_cast<size_t>(MB) * NB * B);
+    double* dQ = c.buf("tune_q", static_cast<size_t>(MB) * NB * B);
+    for (int b = 0; b < B; ++b)
+      ck(cudaMemcpyAsync(dA + static_cast<size_t>(b) * MB * NB, host.data(), host.size() * sizeof(double),
+                         cudaMemcpyHostToDevice, c.stream()));
+    std::vector<const double*> pa(B);
+    std::vector<double*> pq(B);
+    std::vector<int64_t> ld(B, MB);
+    std::vector<int> mm(B, MB), nn(B, NB), inf(B, 0), its(B, 0);
+    for (int b = 0; b < B; ++b) {
+      pa[b] = dA + static_cast<size_t>(b) * MB * NB;
+      pq[b] = dQ + static_cast<size_t>(b) * MB * NB;
+    }
+    double t[2];
+    for (int rep = 0; rep < 2; ++rep) {
+      const int nb_members = rep == 0 ? 1 : B;
+      std::vector<int> idx(nb_members);
+      for (int b = 0; b < nb_members; ++b) idx[b] = b;
+      BatchStats bs;
+      qdwh_bucket(c, idx, MB, NB, mm.data(), nn.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
+                  nullptr, inf.data(), its.data(), &bs);  // warm-up (workspace)
+      EventTimer tm(c.stream());
+      qdwh_bucket(c, idx, MB, NB, mm.data(), nn.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
+                  nullptr, inf.data(), its.data(), &bs);
+      t[rep] = tm.stop();
+    }
+    const double w = std::max(1e-3, (t[1] - t[0]) / (B - 1));
+    lat[k] = std::max(0.0, t[0] - w);
+    flops_at[k] = batch_member_flops(MB, NB);
+    rate[k] = flops_at[k] / w / 1e9;  // TFLOP/s
+  }
+  BatchCostModel md = c.batch_model;
+  // latency: least-squares line in NB/32 through the three probes
+  double sx = 0, sy = 0, sxx = 0, sxy = 0;
+  for (int k = 0; k < 3; ++k) {
+    const double x = sizes[k] / 32.0;
+    sx += x;
+    sy += lat[k];
+    sxx += x * x;
+    sxy += x * lat[k];
+  }
+  const double den = 3.0 * sxx - sx * sx;
+  md.lat1 = std::max(0.0, (3.0 * sxy - sx * sy) / den);
+  md.lat0 = std::max(0.0, (sy - md.lat1 * sx) / 3.0);
+  // rate(NB) = R NB / (NB + h) through the two larger probes
+  const double n1 = sizes[1], n2 = sizes[2], r1 = rate[1], r2 = rate[2];
+  const double h = (r2 - r1) / (r1 / n1 - r2 / n2);
+  if (std::isfinite(h) && h > 0.0 && r2 > 0.0) {
+    md.nhalf = h;
+    md.rate_tflops = r2 * (n2 + h) / n2;
+  } else if (r2 > 0.0) {
+    md.nhalf = 0.0;
+    md.rate_tflops = r2;
+  }
+  c.batch_model = md;
   return 0;
 }
 

@@ -67,10 +67,15 @@ struct BatchStats {
   double flops = 0.0;       // executed FP64 flops, padding included
   double flops_useful = 0.0;  // the same work counted on the unpadded sizes
   double ms = 0.0;
+  double predicted_ms = 0.0;  // the bucket plan's predicted time (cost model)
 };
 int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* const* dA, const int64_t* lda,
                double* const* dQ, const int64_t* ldq, double* const* dH, const int64_t* ldh, int* info,
                int* iterations, BatchStats* bs);
+
+// Measures the batched solver's cost model on this GPU (probe buckets at three sizes) into
+// c.batch_model; the bucket plan of qdwh_batch uses it.  Returns 0.
+int batch_autotune(Context& c);
 
 // H = (Q^T A + A^T Q)/2
 void form_h(Context& c, int m, int n, const double* dQ, int64_t ldq, const double* dA, int64_t lda, double* dH,
