@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--n", "--matrix-n", dest="n", type=int, default=8192)
     ap.add_argument("--rk", type=int, default=8)
     ap.add_argument("--kappa", type=float, default=1e12)
+    ap.add_argument("--no-extras", action="store_true", help="skip the batch and Zolo-SVD configurations")
     ap.add_argument("--ref-timeout", type=float, default=1650.0,
                     help="seconds allowed for the reference arm's one full CPU solve")
     return ap.parse_args()
@@ -329,6 +330,111 @@ def accuracy(torch, dA, dQ, dH, s_true=None) -> dict:
     return out
 
 
+def haar_np(rng, m: int, n: int):
+    q, r = np.linalg.qr(rng.standard_normal((m, n)))
+    return q * np.sign(np.diag(r))[None, :]
+
+
+def bench_batch_c4(torch, zb, h, reps: int = 3) -> dict:
+    """Configuration 4: 512 matrices, n log-uniform in [64, 1024], m = n (1 + U[0,1]), kappa
+    log-uniform in [1e2, 1e14], s geometric; PCG64 seed 1004 (sizes, kappa) and 1004 + i
+    (member i's Haar factors).  One zolo_qdwh_batch_dev call per timed repetition; the worst
+    member's backward error and orthogonality over 10 n eps."""
+    rng = np.random.default_rng(1004)
+    mats = []
+    for i in range(512):
+        n = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        m = int(round(n * (1 + rng.uniform(0, 1))))
+        kappa = 10 ** rng.uniform(2, 14)
+        s = np.geomspace(1.0, 1.0 / kappa, n)
+        r2 = np.random.default_rng(1004 + i)
+        a = np.asfortranarray((haar_np(r2, m, n) * s[None, :]) @ haar_np(r2, n, n).T)
+        mats.append((a, s))
+    da = [torch.from_numpy(a.T.copy()).to("cuda") for a, _ in mats]
+    dq = [torch.empty_like(x) for x in da]
+    dh = [torch.empty((a.shape[1], a.shape[1]), dtype=torch.float64, device="cuda") for a, _ in mats]
+    members = [(a.shape[0], a.shape[1], x.data_ptr(), a.shape[0], q.data_ptr(), a.shape[0], hh.data_ptr(),
+                a.shape[1]) for (a, _), x, q, hh in zip(mats, da, dq, dh)]
+    stream = torch.cuda.current_stream()
+    zb.qdwh_batch_dev(h, members)  # warm-up: workspace of the worker streams
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        info, its = zb.qdwh_batch_dev(h, members)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    st = h.stats()
+    worst_b = worst_o = worst_s = 0.0
+    for (a, s), x, q, hh in zip(mats, da, dq, dh):
+        n = a.shape[1]
+        A, Q, H = x.T, q.T, hh.T
+        be = float(torch.linalg.norm(A - Q @ H) / torch.linalg.norm(A))
+        orth = float(torch.linalg.norm(Q.T @ Q - torch.eye(n, dtype=torch.float64, device="cuda")) / math.sqrt(n))
+        ev = torch.sort(torch.linalg.eigvalsh(0.5 * (H + H.T)), descending=True).values
+        sv = float(torch.max(torch.abs(ev - torch.from_numpy(s).to("cuda"))))
+        tol = 10 * n * 2.220446049250313e-16
+        worst_b, worst_o, worst_s = max(worst_b, be / tol), max(worst_o, orth / tol), max(worst_s, sv)
+    out = {"workload": "512 matrices, n in [64, 1024] log-uniform, m in [n, 2n], kappa in [1e2, 1e14], QDWH-PD "
+                       "batched (zolo_qdwh_batch_dev)", "ms": ms, "matrices_per_s": 512 / (ms * 1e-3), "reps": reps,
+           "info_nonzero": int(sum(1 for v in info if v)), "max_iterations": int(max(its)),
+           "tflops_useful": st["flops"] / (ms * 1e-3) / 1e12,
+           "tflops_executed": st["flops_executed"] / (ms * 1e-3) / 1e12,
+           "worst_backward_error_over_10neps": worst_b, "worst_orthogonality_over_10neps": worst_o,
+           "worst_sv_err_rel_smax": worst_s}
+    del da, dq, dh
+    torch.cuda.empty_cache()
+    return out
+
+
+def bench_svd_c5(torch, zb, h) -> dict:
+    """Configuration 5: Zolo-SVD of a 16384 x 8192 matrix, kappa = 1e10: 70 % of s geometric in
+    [1e-10, 1], 20 % exactly 1, 10 % in clusters of relative gap 1e-9; Gaussians from PCG64 seed
+    1005, their QR (Haar factors) on the GPU.  One zolo_svd_dev call (Zolo-PD r = 8, FP64 fast
+    form, then the spectral divide-and-conquer eigensolver on H)."""
+    m, n = 16384, 8192
+    rng = np.random.default_rng(1005)
+    n70, n20 = int(0.7 * n), int(0.2 * n)
+    n10 = n - n70 - n20
+    base = np.geomspace(1e-1, 1e-9, n10 // 8 + 1)
+    clus = (base[:, None] * (1 + 1e-9 * np.arange(8))[None, :]).reshape(-1)[:n10]
+    s = np.sort(np.concatenate([np.geomspace(1.0, 1e-10, n70), np.ones(n20), clus]))[::-1].copy()
+
+    def haar_gpu(r, c):
+        g = torch.from_numpy(rng.standard_normal((c, r)).T.copy()).to("cuda")
+        q, rr = torch.linalg.qr(g)
+        return q * torch.sign(torch.diagonal(rr))[None, :]
+    u = haar_gpu(m, n)
+    v = haar_gpu(n, n)
+    st = torch.from_numpy(s).to("cuda")
+    a = (u * st[None, :]) @ v.T
+    del u, v
+    da = a.T.contiguous()
+    du = torch.empty_like(da)
+    ds = torch.empty(n, dtype=torch.float64, device="cuda")
+    dv = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    zb.svd_dev(h, m, n, da.data_ptr(), m, du.data_ptr(), m, ds.data_ptr(), dv.data_ptr(), n, algo=1, rk=8)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    U, V = du.T, dv.T
+    eye = torch.eye(n, dtype=torch.float64, device="cuda")
+    out = {"workload": "Zolo-SVD 16384 x 8192, kappa 1e10, 20 % sigma = 1, clusters of gap 1e-9 (zolo_svd_dev, "
+                       "Zolo-PD r = 8 FP64 fast form + spectral divide-and-conquer)",
+           "s": e0.elapsed_time(e1) / 1e3,
+           "residual": float(torch.linalg.norm(a - (U * ds[None, :]) @ V.T) / torch.linalg.norm(a)),
+           "sv_err_rel_smax": float(torch.max(torch.abs(torch.sort(ds, descending=True).values - st)) / st[0]),
+           "orth_u": float(torch.linalg.norm(U.T @ U - eye) / math.sqrt(n)),
+           "orth_v": float(torch.linalg.norm(V.T @ V - eye) / math.sqrt(n))}
+    del a, da, du, dv, eye
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_gpu(args):
     import torch
     # options of the library's default handle (the one the reference-named host-array entry
@@ -474,6 +580,17 @@ def run_gpu(args):
         e2e_call()
     e2e_s = max_over_ranks(dist, (time.perf_counter() - w0) / e2e_steps, "cuda")
     st_e2e = zb.DefaultHandle().stats()
+    zb.lib().zolo_release_workspace(zb.DefaultHandle().ptr)
+    # the other configurations, on one GPU: the 512-matrix batch and the full Zolo-SVD
+    extras = {}
+    if world == 1 and not args.no_extras:
+        set_form("fp64")
+        for name, fn in (("batch_c4", bench_batch_c4), ("svd_c5", bench_svd_c5)):
+            try:
+                extras[name] = fn(torch, zb, h)
+            except Exception as exc:  # an extra must not hide the headline line
+                extras[name] = {"error": str(exc)[:300]}
+            h.release()
     q_e2e = torch.from_numpy(hQ.numpy()).to("cuda")
     eye = torch.eye(n, dtype=torch.float64, device="cuda")
     e2e_orth = float(torch.linalg.norm(q_e2e.T @ q_e2e - eye) / math.sqrt(n))  # Q^T Q (transposes cancel)
@@ -547,6 +664,7 @@ def run_gpu(args):
                     "call": "pzolopd1_ (gfortran symbol) on pinned host arrays, default handle with ZOLO_FAST=1 "
                             "ZOLO_OPT_MIXED=1 from the environment; returns Q (PZOLOPD1 forms no H)",
                     "steps": e2e_steps, "branches": st_e2e["branches"], "orthogonality": e2e_orth},
+            "configs": extras,
             "gpu_launches": int(total_launches),
             "clocks": ck,
             "cpu_baseline": {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",

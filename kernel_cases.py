@@ -19,6 +19,8 @@ solve (e.g. ``ncu -k regex:dgemm_kernel ... python kernel_cases.py --case gemm_n
   oz_k128      C -= A B, M = N = n, K = 128, emulated (the block-reflector update shape)
   oz_m512      P = V^T W, M = 512, N = K = n, emulated (four batched 128-row projections)
   gemm_m512    the same on the DMMA GEMM
+  polar        one Zolo-PD solve (bounds + PZOLOPD1 + H, zolo_polar_dev, FP64 fast form), kappa 1e12
+  polar_mixed  the same in the mixed form (ZOLO_OPT_MIXED = 1)
 
   python kernel_cases.py --case gemm_nn --n 4096 --reps 3
 """
@@ -44,7 +46,8 @@ def load_pkg():
     return mod
 
 
-CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf", "oz_nn", "oz_syrk", "oz_k128", "oz_m512", "gemm_m512")
+CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf", "oz_nn", "oz_syrk", "oz_k128",
+         "oz_m512", "gemm_m512", "polar", "polar_mixed")
 
 
 def main() -> int:
@@ -93,6 +96,26 @@ def main() -> int:
                                     c.data_ptr(), M, tri, 0)
             if rc:
                 raise zb.ZoloError("zolo_dgemm_dev", rc)
+    elif args.case in ("polar", "polar_mixed"):
+        # A = U diag(s) V^T, s log-uniform in [1e-12, 1] (endpoints pinned), Haar U, V
+        def haar():
+            q, r = torch.linalg.qr(randn(n, n))
+            return q * torch.sign(torch.diagonal(r))[None, :]
+        e = torch.rand(n, generator=g, **f64) * -12.0
+        e[0], e[-1] = 0.0, -12.0
+        sv = torch.sort(10.0 ** e, descending=True).values
+        u, v = haar(), haar()
+        a = ((u * sv[None, :]) @ v.T).T.contiguous()  # column-major storage of A
+        del u, v
+        q = torch.empty_like(a)
+        hh = torch.empty_like(a)
+        for opt in (zb.OPT_SHARED_QR, zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_BETA_FROB, zb.OPT_TERM_PLAN):
+            h.set_option(opt, 1)
+        h.set_option(zb.OPT_MIXED, 1 if args.case == "polar_mixed" else 0)
+        flops = 0.0
+
+        def run():
+            zb.polar_dev(h, 8, n, n, a.data_ptr(), n, q.data_ptr(), n, hh.data_ptr(), n)
     elif args.case in ("oz_k128", "oz_m512", "gemm_m512"):
         if args.case == "oz_k128":
             M, N, K, ta, alpha, beta = n, n, 128, b"N", -1.0, 1.0
@@ -161,7 +184,8 @@ def main() -> int:
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        print(f"{args.case} n={n} rep {i}: {ms:.3f} ms, {flops / (ms * 1e-3) / 1e12:.2f} TFLOP/s", flush=True)
+        rate = f", {flops / (ms * 1e-3) / 1e12:.2f} TFLOP/s" if flops else ""
+        print(f"{args.case} n={n} rep {i}: {ms:.3f} ms{rate}", flush=True)
     h.close()
     return 0
 

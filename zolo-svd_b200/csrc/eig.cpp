@@ -6,8 +6,11 @@
 #include "eig.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <mutex>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "linalg.h"
@@ -21,9 +24,11 @@ inline int64_t even(int64_t x) { return (x + 1) / 2 * 2; }
 
 struct DevMem {
   std::vector<void*> ptrs;
+  std::mutex mu;  // nodes of one level are split by concurrent workers
   double* alloc(size_t elems) {
     void* p = nullptr;
     ck(cudaMalloc(&p, std::max<size_t>(elems, 1) * sizeof(double)));
+    std::lock_guard<std::mutex> lk(mu);
     ptrs.push_back(p);
     return static_cast<double*>(p);
   }
@@ -80,6 +85,134 @@ double split_residual(Context& c, int n, int k, const double* H, int64_t ldh, co
   return std::sqrt(d2h(c, c.dscal() + 8));
 }
 
+// Runs task(ctx, i) for i in [0, count): on `c` itself for one task, otherwise on up to four
+// worker contexts (own stream and workspace each, one host thread each) that take the tasks
+// in order.  Work queued on c.stream() before the call is visible to the tasks, and their work
+// is ordered before anything queued on c.stream() after it.  Rethrows a task's CUDA failure.
+template <class F>
+void run_concurrent(Context& c, int count, F&& task) {
+  if (count <= 0) return;
+  const int W = std::min(count, 4);
+  if (W == 1) {
+    for (int i = 0; i < count; ++i) task(c, i);
+    return;
+  }
+  while (static_cast<int>(c.workers.size()) < W) c.workers.emplace_back(new Context(c.device()));
+  ck(cudaEventRecord(c.event(0), c.stream()));
+  std::atomic<int> next{0};
+  std::vector<cudaError_t> err(W, cudaSuccess);
+  std::vector<std::thread> th;
+  for (int w = 0; w < W; ++w) {
+    th.emplace_back([&, w] {
+      try {
+        Context& wc = *c.workers[w];
+        ck(cudaSetDevice(wc.device()));
+        ck(cudaStreamWaitEvent(wc.stream(), c.event(0), 0));
+        wc.zolo_mixed = c.zolo_mixed;
+        wc.oz_slices = c.oz_slices;
+        for (int i = next++; i < count; i = next++) task(wc, i);
+      } catch (const CudaFailure& e) {
+        err[w] = e.err;
+        next = count;
+      } catch (...) {
+        err[w] = cudaErrorUnknown;
+        next = count;
+      }
+    });
+  }
+  for (auto& t : th) t.join();
+  for (int w = 0; w < W; ++w) {
+    Context& wc = *c.workers[w];
+    ck(cudaEventRecord(wc.event(0), wc.stream()));
+    ck(cudaStreamWaitEvent(c.stream(), wc.event(0), 0));
+  }
+  for (int w = 0; w < W; ++w)
+    if (err[w] != cudaSuccess) throw CudaFailure{err[w]};
+}
+
+// One node of the divide-and-conquer: a leaf (m <= kJacobiLeaf) or a split into the blocks of
+// V^T H V above and below a shift (QDWH polar factor of H - sigma I, subspace basis of its
+// projector).  Fills nd (k, V, Z, w) and the children L, R; returns false if no candidate
+// shift splits the spectrum.
+bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnorm, uint64_t seed, EigStats& S) {
+  const double eps = 2.220446049250313e-16;
+  const int m = nd.n;
+  const int64_t ldm = even(m);
+  nd.Z = mem.alloc(static_cast<size_t>(ldm) * m);
+  nd.w = mem.alloc(m);
+  if (m <= kJacobiLeaf) {
+    nd.leaf = true;
+    return true;
+  }
+  // split points: median and mean of the diagonal, then nudged versions
+  std::vector<double> dg(m);
+  double* dd = c.buf("eig_diag", m);
+  ck(get_diag(m, nd.H, nd.ld, dd, c.stream()));
+  ck(cudaMemcpyAsync(dg.data(), dd, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream()));
+  ck(cudaStreamSynchronize(c.stream()));
+  std::vector<double> srt = dg;
+  std::sort(srt.begin(), srt.end());
+  const double med = srt[m / 2], mean = std::accumulate(dg.begin(), dg.end(), 0.0) / m;
+  const double span = std::max(srt.back() - srt.front(), 1e-300);
+  const double cand[4] = {0.5 * (srt[(m - 1) / 2] + srt[m / 2]), mean, med + 1e-3 * span, med - 1e-3 * span};
+  nd.V = mem.alloc(static_cast<size_t>(ldm) * m);
+  double* Up = c.buf("eig_up", static_cast<size_t>(ldm) * m);
+  double* P = c.buf("eig_p", static_cast<size_t>(ldm) * m);
+  double* X = c.buf("eig_x", static_cast<size_t>(ldm) * m);
+  double* E = c.buf("eig_e", static_cast<size_t>(ldm) * m);
+  for (int a = 0; a < 4; ++a) {
+    QdwhOpts o;
+    o.sym = 'N';
+    o.sigma = cand[a];
+    o.bounds = BOUNDS_PQDWHFACS;
+    o.maxit = 12;
+    const Stats saved = c.stats;
+    const int info = qdwh(c, m, m, nd.H, nd.ld, Up, ldm, nullptr, 0, o);
+    S.qdwh_calls++;
+    S.qdwh_iterations += c.stats.iterations;
+    S.flops += c.stats.flops;
+    c.stats = saved;
+    if (info != 0) continue;
+    // projector onto the eigenvalues above the split: P = (Up + I)/2, k = trace(P)
+    ck(scale_copy(m, m, 0.5, Up, ldm, 0, P, ldm, 0, 1, 0.5, c.stream()));
+    ck(trace(m, P, ldm, c.dscal() + 10, c.stream()));
+    const int k = static_cast<int>(std::lround(d2h(c, c.dscal() + 10)));
+    if (k <= 0 || k >= m) continue;
+    // subspace: V = full Q of QR(P * Omega); a second pass with X = P V1 if the split leaks
+    double* Om = c.buf("eig_om", static_cast<size_t>(ldm) * k);
+    ck(fill_random(m, k, Om, ldm, seed + a, c.stream()));
+    gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{Om, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
+    basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
+    const double tol = 10.0 * eps * std::sqrt(static_cast<double>(m)) * std::max(hnorm, 1e-300);
+    double off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
+    S.subspace_passes++;
+    for (int pass = 1; pass < 3 && off > tol; ++pass) {
+      gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{nd.V, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
+      basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
+      off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
+      S.subspace_passes++;
+    }
+    S.max_split_residual = std::max(S.max_split_residual, off / std::max(hnorm, 1e-300));
+    nd.k = k;
+    L = Node{};
+    R = Node{};
+    L.n = k;
+    L.ld = even(k);
+    L.H = mem.alloc(static_cast<size_t>(L.ld) * k);
+    ck(scale_copy(k, k, 1.0, E, ldm, 0, L.H, L.ld, 0, 1, 0.0, c.stream()));
+    ck(symmetrize(k, L.H, L.ld, c.stream()));
+    R.n = m - k;
+    R.ld = even(m - k);
+    R.H = mem.alloc(static_cast<size_t>(R.ld) * (m - k));
+    ck(scale_copy(m - k, m - k, 1.0, E + k + static_cast<int64_t>(k) * ldm, ldm, 0, R.H, R.ld, 0, 1, 0.0,
+                  c.stream()));
+    ck(symmetrize(m - k, R.H, R.ld, c.stream()));
+    S.splits++;
+    return true;
+  }
+  return false;
+}
+
 }  // namespace
 
 int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz, EigStats* es) {
@@ -100,94 +233,42 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   double hnorm;
   ck(frob2(n, n, nodes[0].H, nodes[0].ld, c.dpartial(), c.dscal() + 9, c.stream()));
   hnorm = std::sqrt(d2h(c, c.dscal() + 9));
-  // accepted leak ||V2^T H V1||_F of a split (the dropped block is the eigen-residual it adds)
-  const double eps = 2.220446049250313e-16;
 
-  // ---- top-down splits ----
-  for (size_t ni = 0; ni < nodes.size(); ++ni) {
-    Node nd = nodes[ni];
-    const int m = nd.n;
-    const int64_t ldm = even(m);
-    nd.Z = mem.alloc(static_cast<size_t>(ldm) * m);
-    nd.w = mem.alloc(m);
-    if (m <= kJacobiLeaf) {
-      nd.leaf = true;
-      nodes[ni] = nd;
-      continue;
+  // ---- top-down splits, one level at a time: the nodes of a level run concurrently ----
+  std::vector<std::pair<size_t, size_t>> levels;
+  for (size_t lo = 0; lo < nodes.size();) {
+    const size_t hi = nodes.size();
+    levels.emplace_back(lo, hi);
+    const int cnt = static_cast<int>(hi - lo);
+    std::vector<Node> kids(2 * cnt);
+    std::vector<EigStats> st(cnt);
+    std::vector<char> ok(cnt, 1);
+    run_concurrent(c, cnt, [&](Context& wc, int i) {
+      ok[i] = split_node(wc, nodes[lo + i], kids[2 * i], kids[2 * i + 1], mem, hnorm,
+                         0x5EEDull + (lo + i) * 7919ull, st[i]) ? 1 : 0;
+    });
+    for (int i = 0; i < cnt; ++i) {
+      S.qdwh_calls += st[i].qdwh_calls;
+      S.qdwh_iterations += st[i].qdwh_iterations;
+      S.subspace_passes += st[i].subspace_passes;
+      S.splits += st[i].splits;
+      S.flops += st[i].flops;
+      S.max_split_residual = std::max(S.max_split_residual, st[i].max_split_residual);
     }
-    // split points: median and mean of the diagonal, then nudged versions
-    std::vector<double> dg(m);
-    double* dd = c.buf("eig_diag", m);
-    ck(get_diag(m, nd.H, nd.ld, dd, c.stream()));
-    ck(cudaMemcpyAsync(dg.data(), dd, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream()));
-    ck(cudaStreamSynchronize(c.stream()));
-    std::vector<double> srt = dg;
-    std::sort(srt.begin(), srt.end());
-    const double med = srt[m / 2], mean = std::accumulate(dg.begin(), dg.end(), 0.0) / m;
-    const double span = std::max(srt.back() - srt.front(), 1e-300);
-    const double cand[4] = {0.5 * (srt[(m - 1) / 2] + srt[m / 2]), mean, med + 1e-3 * span, med - 1e-3 * span};
-    nd.V = mem.alloc(static_cast<size_t>(ldm) * m);
-    double* Up = c.buf("eig_up", static_cast<size_t>(ldm) * m);
-    double* P = c.buf("eig_p", static_cast<size_t>(ldm) * m);
-    double* X = c.buf("eig_x", static_cast<size_t>(ldm) * m);
-    double* E = c.buf("eig_e", static_cast<size_t>(ldm) * m);
-    bool ok = false;
-    for (int a = 0; a < 4 && !ok; ++a) {
-      QdwhOpts o;
-      o.sym = 'N';
-      o.sigma = cand[a];
-      o.bounds = BOUNDS_PQDWHFACS;
-      o.maxit = 12;
-      const Stats saved = c.stats;
-      const int info = qdwh(c, m, m, nd.H, nd.ld, Up, ldm, nullptr, 0, o);
-      S.qdwh_calls++;
-      S.qdwh_iterations += c.stats.iterations;
-      S.flops += c.stats.flops;
-      c.stats = saved;
-      if (info != 0) continue;
-      // projector onto the eigenvalues above the split: P = (Up + I)/2, k = trace(P)
-      ck(scale_copy(m, m, 0.5, Up, ldm, 0, P, ldm, 0, 1, 0.5, c.stream()));
-      ck(trace(m, P, ldm, c.dscal() + 10, c.stream()));
-      const int k = static_cast<int>(std::lround(d2h(c, c.dscal() + 10)));
-      if (k <= 0 || k >= m) continue;
-      // subspace: V = full Q of QR(P * Omega); a second pass with X = P V1 if the split leaks
-      double* Om = c.buf("eig_om", static_cast<size_t>(ldm) * k);
-      ck(fill_random(m, k, Om, ldm, 0x5EEDull + ni * 7919ull + a, c.stream()));
-      gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{Om, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
-      basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
-      const double tol = 10.0 * eps * std::sqrt(static_cast<double>(m)) * std::max(hnorm, 1e-300);
-      double off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
-      S.subspace_passes++;
-      for (int pass = 1; pass < 3 && off > tol; ++pass) {
-        gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{nd.V, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
-        basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
-        off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
-        S.subspace_passes++;
-      }
-      S.max_split_residual = std::max(S.max_split_residual, off / std::max(hnorm, 1e-300));
-      nd.k = k;
-      Node L, R;
-      L.n = k;
-      L.ld = even(k);
-      L.H = mem.alloc(static_cast<size_t>(L.ld) * k);
-      ck(scale_copy(k, k, 1.0, E, ldm, 0, L.H, L.ld, 0, 1, 0.0, c.stream()));
-      ck(symmetrize(k, L.H, L.ld, c.stream()));
-      R.n = m - k;
-      R.ld = even(m - k);
-      R.H = mem.alloc(static_cast<size_t>(R.ld) * (m - k));
-      ck(scale_copy(m - k, m - k, 1.0, E + k + static_cast<int64_t>(k) * ldm, ldm, 0, R.H, R.ld, 0, 1, 0.0,
-                    c.stream()));
-      ck(symmetrize(m - k, R.H, R.ld, c.stream()));
+    for (int i = 0; i < cnt; ++i)
+      if (!ok[i]) return 2;  // no usable split point (all candidates failed)
+    for (int i = 0; i < cnt; ++i) {
+      Node& nd = nodes[lo + i];
+      if (nd.leaf) continue;
       nd.left = static_cast<int>(nodes.size());
       nd.right = nd.left + 1;
-      nodes[ni] = nd;
-      nodes.push_back(L);
-      nodes.push_back(R);
-      S.splits++;
-      ok = true;
+      nodes.push_back(kids[2 * i]);
+      nodes.push_back(kids[2 * i + 1]);
     }
-    if (!ok) return 2;  // no usable split point (all candidates failed)
-    if (ni != 0) mem.release(nodes[ni].H);
+    // the split nodes' matrices are no longer needed (freed between levels: cudaFree waits)
+    for (size_t i = lo; i < hi; ++i)
+      if (i != 0 && !nodes[i].leaf) mem.release(nodes[i].H);
+    lo = hi;
   }
 
   // ---- leaves: one batched Jacobi launch ----
@@ -208,20 +289,28 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     for (int s : sw) S.max_jacobi_sweeps = std::max(S.max_jacobi_sweeps, s);
   }
 
-  // ---- bottom-up back-transformation ----
-  for (int ni = static_cast<int>(nodes.size()) - 1; ni >= 0; --ni) {
-    Node& nd = nodes[ni];
-    if (nd.leaf) continue;
-    const Node& L = nodes[nd.left];
-    const Node& R = nodes[nd.right];
-    const int m = nd.n, k = nd.k;
-    const int64_t ldm = even(m);
-    gemm(c, 0, 0, m, k, k, 1.0, Mat{nd.V, ldm, 0}, Mat{L.Z, even(L.n), 0}, 0.0, Mat{nd.Z, ldm, 0}, 1);
-    gemm(c, 0, 0, m, m - k, m - k, 1.0, Mat{nd.V + static_cast<int64_t>(k) * ldm, ldm, 0}, Mat{R.Z, even(R.n), 0},
-         0.0, Mat{nd.Z + static_cast<int64_t>(k) * ldm, ldm, 0}, 1);
-    ck(cudaMemcpyAsync(nd.w, L.w, sizeof(double) * k, cudaMemcpyDeviceToDevice, c.stream()));
-    ck(cudaMemcpyAsync(nd.w + k, R.w, sizeof(double) * (m - k), cudaMemcpyDeviceToDevice, c.stream()));
-    S.flops += 2.0 * m * (static_cast<double>(k) * k + static_cast<double>(m - k) * (m - k));
+  // ---- bottom-up back-transformation, one level at a time (concurrent within a level) ----
+  for (auto lv = levels.rbegin(); lv != levels.rend(); ++lv) {
+    const size_t lo = lv->first;
+    const int cnt = static_cast<int>(lv->second - lv->first);
+    run_concurrent(c, cnt, [&](Context& wc, int i) {
+      Node& nd = nodes[lo + i];
+      if (nd.leaf) return;
+      const Node& L = nodes[nd.left];
+      const Node& R = nodes[nd.right];
+      const int m = nd.n, k = nd.k;
+      const int64_t ldm = even(m);
+      gemm(wc, 0, 0, m, k, k, 1.0, Mat{nd.V, ldm, 0}, Mat{L.Z, even(L.n), 0}, 0.0, Mat{nd.Z, ldm, 0}, 1);
+      gemm(wc, 0, 0, m, m - k, m - k, 1.0, Mat{nd.V + static_cast<int64_t>(k) * ldm, ldm, 0},
+           Mat{R.Z, even(R.n), 0}, 0.0, Mat{nd.Z + static_cast<int64_t>(k) * ldm, ldm, 0}, 1);
+      ck(cudaMemcpyAsync(nd.w, L.w, sizeof(double) * k, cudaMemcpyDeviceToDevice, wc.stream()));
+      ck(cudaMemcpyAsync(nd.w + k, R.w, sizeof(double) * (m - k), cudaMemcpyDeviceToDevice, wc.stream()));
+    });
+    for (int i = 0; i < cnt; ++i) {
+      const Node& nd = nodes[lo + i];
+      if (!nd.leaf)
+        S.flops += 2.0 * nd.n * (static_cast<double>(nd.k) * nd.k + static_cast<double>(nd.n - nd.k) * (nd.n - nd.k));
+    }
   }
 
   // ---- ascending order (dsyevd / ELPA convention) ----
