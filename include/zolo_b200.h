@@ -361,6 +361,23 @@ int zolo_zolochol_dev(zolo_handle_t h, int m, int n, const double* dX, int64_t l
 int zolo_formx2_dev(zolo_handle_t h, int m, int n, double fone, double* dX, int64_t ldx, const double* dZ,
                     int64_t ldz, double* err);
 
+/* ---- MatrixMarket input (prepare_matrix.f90:154-321 prepare_real_GEM, :638-759
+ * prepare_real_symm_MM), host only ----
+ * Reads the MatrixMarket file `path` (coordinate or array; real, double or integer values)
+ * into the column-major m x n host matrix a (leading dimension lda >= m), zero where no entry
+ * is given.  A `symmetric` file (one triangle stored) yields the full matrix A + A^T with the
+ * diagonal halved, as the reference builds it; a `general` file is used as stored; any other
+ * symmetry class is loaded as stored and reported as ZOLO_MM_OTHER.  With a = NULL only the
+ * header is read (m, n, kind).  kind may be NULL.  The reference's sigma is 0 (its diagonal
+ * shift is commented out, prepare_matrix.f90:260), so no shift is applied.  Returns 0; -1 a
+ * null argument, -6 lda < m, -10 the file cannot be opened, -11 not a MatrixMarket matrix
+ * banner, -12 neither coordinate nor array, -13 complex or pattern values, -14 a bad size
+ * line, -15 too few entries, -16 an index out of range, -17 a non-square symmetric file. */
+#define ZOLO_MM_GENERAL 0
+#define ZOLO_MM_SYMMETRIC 1
+#define ZOLO_MM_OTHER 2
+int zolo_read_mm(const char* path, int* m, int* n, int* kind, double* a, int64_t lda);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ----
  * Lower Cholesky in place of an n x n SPD matrix on the caller's stream, with no
  * device allocation and no handle: for callers that cannot let a library call

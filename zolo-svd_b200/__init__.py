@@ -125,6 +125,7 @@ _SIGS = [
     ("zolo_batch_set_model", C.c_int, [C.c_void_p, c_double_p]),
     ("zolo_batch_plan", C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p,
                                   c_int_p, c_double_p]),
+    ("zolo_read_mm", C.c_int, [C.c_char_p, c_int_p, c_int_p, c_int_p, c_double_p, C.c_int64]),
     ("zolo_dpotrf_dev", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
     ("zolo_dtrsm_dev", C.c_int, [C.c_void_p, C.c_char, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                  C.c_int64, C.c_void_p, C.c_int64]),
@@ -333,6 +334,23 @@ def batch_plan(m, n, model=None, max_batch: int = 1024, mode: int = 0):
     if r < 0:
         raise ZoloError("zolo_batch_plan", r)
     return bucket, [(int(mb[b]), int(nb[b])) for b in range(r)], pred.value
+
+
+MM_KINDS = {0: "general", 1: "symmetric", 2: "other"}
+
+
+def read_mm(path: str):
+    """A MatrixMarket file as a dense Fortran-order matrix, the reference's way
+    (prepare_real_GEM / prepare_real_symm_MM): returns (A, kind)."""
+    m, n, kind = C.c_int(), C.c_int(), C.c_int()
+    r = lib().zolo_read_mm(path.encode(), C.byref(m), C.byref(n), C.byref(kind), None, 1)
+    if r != 0:
+        raise ZoloError("zolo_read_mm", r)
+    a = np.zeros((m.value, n.value), order="F")
+    r = lib().zolo_read_mm(path.encode(), C.byref(m), C.byref(n), C.byref(kind), _dp(a), max(1, m.value))
+    if r != 0:
+        raise ZoloError("zolo_read_mm", r)
+    return a, MM_KINDS[kind.value]
 
 
 def pzolopd_f77(sym: str, rk: int, m: int, n: int, alpha: float, beta: float, a_ptr: int, lda: int, q_ptr: int,
