@@ -163,6 +163,14 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * not numerically positive definite (the reference ignores PDPOSV's INFO).  Host-side only:
  * no kernel is made to fail. */
 #define ZOLO_OPT_INJECT_CHOL_FAIL 9
+/* ZOLO_OPT_NORM2_BOUND: 0 (default) = zolo_polar_dev scales by ALPHA = ||A||_F; 1 = ALPHA
+ * is lowered to a guaranteed upper bound of ||A||_2 (zolo_bounds_dev mode 3): the power method
+ * by repeated squaring of R^T R (R of A/||A||_F), ALPHA = ||A||_F ||(R^T R)^4||_F^(1/8)
+ * (1 + 1e-4) = (sum_i sigma_i^16)^(1/16) (1 + 1e-4) >= sigma_max, capped by ||A||_F; BETA is
+ * rescaled with it, so the iterate is unchanged and CON = 1/BETA is smaller by ||A||_F/ALPHA.
+ * 7n^3/3 extra flops.  The intent of the reference's pdnormest (pdnormest.f90:44-79, a power
+ * iteration for ||A||_2).  No reference counterpart as an option. */
+#define ZOLO_OPT_NORM2_BOUND 10
 /* The default handle (used by the reference-named host-array entry points) reads its options
  * from the environment when it is created, so an unchanged Fortran driver selects them:
  * ZOLO_FAST=1 sets ZOLO_OPT_SHARED_QR, _NS_FINISH, _CHOL_INVERSE, _BETA_FROB, _TERM_PLAN and
@@ -298,7 +306,9 @@ int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double al
 /* The driver's bounds (test_zolodrv1.f90:167-189 replaced by a QR + R^{-1} estimate):
  * alpha = ||A||_F, beta = 1/(sqrt(n) ||R^{-1}||_1) for A/alpha = QR (mode 1) or
  * ||A/alpha||_1 / (sqrt(n) ||R^{-1}||_1) (mode 0), or 1/||R^{-1}||_F (mode 2: still a
- * lower bound on sigma_min(A/alpha), and never below mode 1's).  Returns -7 for another mode. */
+ * lower bound on sigma_min(A/alpha), and never below mode 1's); mode 3: alpha is the
+ * guaranteed ||A||_2 upper bound of ZOLO_OPT_NORM2_BOUND and beta mode 2's bound rescaled to
+ * A/alpha (sigma(A/alpha) lies in [beta, 1]).  Returns -7 for another mode. */
 int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* dA, int64_t lda, int mode,
                     double* alpha, double* beta);
 /* H = (Q^T A + A^T Q)/2 (pqdwhfacs.f90:460-466, ZoloCHK1.f90:80-83). */

@@ -542,3 +542,56 @@ def test_matrixmarket_symmetric_through_pqdwhfacs(tmp_path):
     ev = np.abs(np.linalg.eigvalsh(shifted))
     kappa = ev.max() / ev.min()
     assert np.linalg.norm(q - q_o) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
+
+
+def _config_spectra(n, rng):
+    """The five configurations' singular-value shapes at order n (kappa as configured)."""
+    c1 = np.geomspace(1.0, 1e-8, n)
+    c2 = np.geomspace(1.0, 1e-16, n)
+    idx = rng.choice(np.arange(1, n), n // 20, replace=False)
+    c2[idx] = c2[idx - 1]
+    e = rng.uniform(-12, 0, n)
+    e[0], e[-1] = 0.0, -12.0
+    c3 = np.sort(10.0 ** e)[::-1]
+    c4 = np.geomspace(1.0, 1.0 / 10 ** rng.uniform(2, 14), n)
+    n70, n20 = int(0.7 * n), int(0.2 * n)
+    base = np.geomspace(1e-1, 1e-9, (n - n70 - n20) // 8 + 1)
+    clus = (base[:, None] * (1 + 1e-9 * np.arange(8))[None, :]).reshape(-1)[: n - n70 - n20]
+    c5 = np.sort(np.concatenate([np.geomspace(1.0, 1e-10, n70), np.ones(n20), clus]))[::-1]
+    return {"c1": c1, "c2": np.sort(c2)[::-1], "c3": c3, "c4": c4, "c5": c5}
+
+
+@pytest.mark.parametrize("cfg", ["c1", "c2", "c3", "c4", "c5"])
+def test_norm2_upper_bound_on_config_spectra(cfg):
+    """zolo_bounds_dev mode 3: alpha >= sigma_max(A) (a guaranteed bound, within a 16-th root
+    of the spectrum's weight of it, and never above ||A||_F), beta * alpha <= sigma_min(A); the
+    Zolo-PD solve with ZOLO_OPT_NORM2_BOUND takes the smaller CON and stays backward stable."""
+    import torch
+    n = 640
+    rng = np.random.default_rng(hash(cfg) % 1000)
+    s = _config_spectra(n, rng)[cfg] * 3.7  # not normalized: sigma_max = 3.7
+    a, u, v = zo.make_matrix(n, s, 3100 + int(cfg[1]))
+    h = zb.Handle(0)
+    da = zb.colmajor_to_device(a)
+    torch.cuda.synchronize()
+    al3, be3, _ = zb.bounds_dev(h, n, n, da.data_ptr(), n, mode=3)
+    al2, be2, _ = zb.bounds_dev(h, n, n, da.data_ptr(), n, mode=2)
+    smax, smin = s.max(), s.min()
+    assert al3 >= smax and al3 <= al2 * (1 + 1e-12)
+    assert al3 <= smax * n ** (1.0 / 16.0) * 1.001
+    assert be3 * al3 <= smin * (1 + 1e-9) and abs(be3 * al3 - be2 * al2) <= 1e-9 * be2 * al2
+    dq = torch.zeros_like(da)
+    dh = torch.zeros_like(da)
+    for opt in (zb.OPT_SHARED_QR, zb.OPT_NS_FINISH, zb.OPT_CHOL_INVERSE, zb.OPT_BETA_FROB, zb.OPT_TERM_PLAN):
+        h.set_option(opt, 1)
+    cons = []
+    for norm2 in (0, 1):
+        h.set_option(zb.OPT_NORM2_BOUND, norm2)
+        assert zb.polar_dev(h, 8, n, n, da.data_ptr(), n, dq.data_ptr(), n, dh.data_ptr(), n) == 0
+        st = h.stats()
+        cons.append(st["con"][0] if "con" in st else None)
+        q, hh = zb.device_to_colmajor(dq), zb.device_to_colmajor(dh)
+        check_pd(a, q, hh, n)
+    h.close()
+    if cons[0] is not None:
+        assert cons[1] <= cons[0] * (1 + 1e-12)

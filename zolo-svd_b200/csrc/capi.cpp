@@ -131,6 +131,9 @@ int set_option(Context& c, int option, int value) {
       if (value < 0) return -3;
       c.inject_chol_fail = value;
       return 0;
+    case ZOLO_OPT_NORM2_BOUND:
+      c.zolo_norm2 = value != 0;
+      return 0;
     default:
       return -1;
   }
@@ -327,6 +330,7 @@ int zolo_get_option(zolo_handle_t h, int option, int* value) {
       case ZOLO_OPT_MIXED_SLICES: *value = c.oz_slices; return 0;
       case ZOLO_OPT_OWN_BOUNDS: *value = c.zolo_own_bounds; return 0;
       case ZOLO_OPT_INJECT_CHOL_FAIL: *value = c.inject_chol_fail; return 0;
+      case ZOLO_OPT_NORM2_BOUND: *value = c.zolo_norm2; return 0;
       default: return -1;
     }
   });
@@ -547,7 +551,7 @@ int zolo_pzolopd1_dev(zolo_handle_t h, char sym, int rk, int m, int n, double al
 int zolo_bounds_dev(zolo_handle_t h, int m, int n, double sigma, const double* dA, int64_t lda, int mode,
                     double* alpha, double* beta) {
   if (m < n) return -2;
-  if (mode < 0 || mode > 2) return -7;
+  if (mode < 0 || mode > 3) return -7;
   return guarded(h, [&](Context& c) {
     c.stats = zolo::Stats{};
     return zolo::bounds(c, m, n, sigma, dA, lda, static_cast<zolo::BoundsMode>(mode), alpha, beta);

@@ -109,6 +109,8 @@ class Context {
   int zolo_mixed = 0;
   // PZOLOPD1 entries: 1 = compute ALPHA, BETA from A (zolo_polar) instead of the caller's
   int zolo_own_bounds = 0;
+  // zolo_polar's bounds: 1 = alpha lowered to a guaranteed bound of ||A||_2 (BOUNDS_NORM2)
+  int zolo_norm2 = 0;
   // diagnostic: k + 1 = the Cholesky step of iteration k reports failure (0 = off)
   int inject_chol_fail = 0;
   // batched solver: cost model of its bucket plan, and the worker contexts (own stream and

@@ -314,8 +314,36 @@ void form_h(Context& c, int m, int n, const double* dQ, int64_t ldq, const doubl
   c.stats.flops += 2.0 * m * static_cast<double>(n) * n;
 }
 
+namespace {
+// Guaranteed upper bound of ||R||_2 for an upper-triangular n x n R (the factor of A/alpha_F,
+// so ||R||_2 <= ||R||_F = 1): the power method by repeated squaring, G = R^T R, G^2, G^4, and
+// ||G^4||_F^(1/8) = (sum sigma_i^16)^(1/16) >= sigma_max; times 1 + 1e-4 against rounding,
+// capped by 1.  The intent of the reference's broken pdnormest.f90:44-79 (a power iteration
+// for ||A||_2), made a certain bound.  7n^3/3 flops.
+double norm2_upper(Context& c, int n, const double* W, int64_t ldw) {
+  const int64_t ldn = even(n);
+  double* Ru = c.buf("n2_r", static_cast<size_t>(ldn) * n);
+  double* G = c.buf("n2_g", static_cast<size_t>(ldn) * n);
+  double* G2 = c.buf("n2_g2", static_cast<size_t>(ldn) * n);
+  ck(copy_upper(n, W, ldw, 1.0, Ru, ldn, c.stream()));
+  // G = R^T R: op(A) = R^T is lower triangular (k <= row)
+  gemm(c, 1, 0, n, n, n, 1.0, Mat{Ru, ldn, 0}, Mat{Ru, ldn, 0}, 0.0, Mat{G, ldn, 0}, 1, nullptr, 1, 0, nullptr, 1);
+  ck(mirror_lower(n, G, ldn, c.stream()));
+  gemm(c, 0, 0, n, n, n, 1.0, Mat{G, ldn, 0}, Mat{G, ldn, 0}, 0.0, Mat{G2, ldn, 0}, 1, nullptr, 1, 0);
+  ck(mirror_lower(n, G2, ldn, c.stream()));
+  gemm(c, 0, 0, n, n, n, 1.0, Mat{G2, ldn, 0}, Mat{G2, ldn, 0}, 0.0, Mat{G, ldn, 0}, 1, nullptr, 1, 0);
+  ck(mirror_lower(n, G, ldn, c.stream()));
+  ck(frob2(n, n, G, ldn, c.dpartial(), c.dscal() + 5, c.stream()));
+  c.stats.launches += 8;
+  c.stats.flops += 7.0 / 3.0 * static_cast<double>(n) * n * n;
+  const double f = d2h(c, c.dscal() + 5);  // ||G^4||_F^2 = sum sigma^16
+  if (!(f > 0.0) || !std::isfinite(f)) return 1.0;
+  return std::min(1.0, std::pow(f, 1.0 / 16.0) * (1.0 + 1e-4));
+}
+}  // namespace
+
 int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda, BoundsMode mode, double* alpha,
-           double* beta) {
+           double* beta, double* alpha_fro) {
   const int64_t ldx = even(m), ldn = even(n);
   double* X = c.buf("bnd_x", static_cast<size_t>(ldx) * n);
   double* scal = c.dscal();
@@ -325,6 +353,7 @@ int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda
   c.stats.launches += 3;
   const double a = std::sqrt(d2h(c, scal));
   *alpha = a;
+  if (alpha_fro) *alpha_fro = a;
   if (!(a > 0.0) || !std::isfinite(a)) {
     *beta = 0.0;
     return 1;
@@ -365,7 +394,14 @@ int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda
     return 1;
   }
   // sigma_min(X) = 1/||R^{-1}||_2 >= 1/||R^{-1}||_F >= 1/(sqrt(n) ||R^{-1}||_1)
-  *beta = mode == BOUNDS_FROB ? 1.0 / std::sqrt(fr) : temp_beta / (std::sqrt(static_cast<double>(n)) * inv1);
+  *beta = (mode == BOUNDS_FROB || mode == BOUNDS_NORM2) ? 1.0 / std::sqrt(fr)
+                                                        : temp_beta / (std::sqrt(static_cast<double>(n)) * inv1);
+  if (mode == BOUNDS_NORM2) {
+    // A/alpha' with alpha' = alpha s2 >= ||A||_2 has sigma_min >= beta / s2
+    const double s2 = norm2_upper(c, n, X, ldx);
+    *alpha = a * s2;
+    *beta /= s2;
+  }
   return 0;
 }
 
@@ -507,8 +543,10 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
   double* X = c.buf("Xit", static_cast<size_t>(ldx) * n);
   // R with its zeros below the diagonal (the reflectors live there), for H at the end
   double* Rx = factored && dH ? c.buf("zf_r", static_cast<size_t>(even(n)) * n) : nullptr;
+  // X0 = A/(alpha beta) = Q_x R (pf->alpha / (alpha beta)): Y0 = R / ys
+  const double ys = pf ? beta * alpha / pf->alpha : 1.0;
   if (factored) {
-    ck(copy_upper(n, pf->W, pf->ldw, 1.0 / beta, X, ldx, c.stream()));
+    ck(copy_upper(n, pf->W, pf->ldw, 1.0 / ys, X, ldx, c.stream()));
     if (Rx) ck(copy_upper(n, pf->W, pf->ldw, 1.0, Rx, even(n), c.stream()));
     c.stats.launches += 2;
   } else {
@@ -633,7 +671,7 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
       z_summed = shared;
       // the first iteration may reuse the QR of A/alpha: X0 = (A/alpha)/beta
       const Prefactored* pfi = (shared && it == 0) ? pf : nullptr;
-      for (int b = 0; b < rk_it; ++b) hv[b] = std::sqrt(coeff[2 * b]) * (pfi ? beta : 1.0);
+      for (int b = 0; b < rk_it; ++b) hv[b] = std::sqrt(coeff[2 * b]) * (pfi ? ys : 1.0);
       h2d(c, dvec, hv.data(), rk_it);
       for (int b = 0; b < rk_it; ++b) hv[16 + b] = -coeff[2 * rk_it + b] / std::sqrt(coeff[2 * b]);
       if (shared) {
@@ -688,11 +726,12 @@ int zolo_pd(Context& c, char sym, int rk, int m, int n, double alpha, double bet
     const double dm = m, dn = n;
     c.stats.flops_exec_delta += 4.0 * dm * dn * dn - 2.0 * dn * dn * dn;
     if (dH) {
-      // H = sym(Q^T A) = sym(alpha Y^T R) = sym(alpha R^T Y): R^T is lower triangular (k up to the row)
+      // H = sym(Q^T A) = sym(a Y^T R) = sym(a R^T Y), a = pf->alpha (A = a Q_x R): R^T is lower
+      // triangular (k up to the row)
       const int64_t ldh_i = even(n);
       double* Hb = c.buf("Hbuf", static_cast<size_t>(ldh_i) * n);
-      gemm(c, 1, 0, n, n, n, alpha, Mat{Rx, even(n), 0}, Mat{X, ldx, 0}, 0.0, Mat{Hb, ldh_i, 0}, 1, nullptr, 0, 0,
-           nullptr, 1);
+      gemm(c, 1, 0, n, n, n, pf->alpha, Mat{Rx, even(n), 0}, Mat{X, ldx, 0}, 0.0, Mat{Hb, ldh_i, 0}, 1, nullptr, 0,
+           0, nullptr, 1);
       ck(symmetrize(n, Hb, ldh_i, c.stream()));
       ck(scale_copy(n, n, 1.0, Hb, ldh_i, 0, dH, ldh, 0, 1, 0.0, c.stream()));
       c.stats.launches += 2;
@@ -739,9 +778,10 @@ int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, 
   if (rk < 1 || rk > 8) return -2;
   if (m == 0 || n == 0) return 0;
   EventTimer total(c.stream());
-  double alpha = 0.0, beta = 0.0;
+  double alpha = 0.0, beta = 0.0, alpha_fro = 0.0;
   EventTimer tb(c.stream());
-  const int binfo = bounds(c, m, n, 0.0, dA, lda, c.zolo_beta_frob ? BOUNDS_FROB : BOUNDS_ZOLOPD, &alpha, &beta);
+  const BoundsMode bm = c.zolo_norm2 ? BOUNDS_NORM2 : (c.zolo_beta_frob ? BOUNDS_FROB : BOUNDS_ZOLOPD);
+  const int binfo = bounds(c, m, n, 0.0, dA, lda, bm, &alpha, &beta, &alpha_fro);
   const double ms_bounds = tb.stop();
   const double bflops = 4.0 / 3.0 * static_cast<double>(n) * n * n + 2.0 * m * static_cast<double>(n) * n;
   if (binfo != 0) {
@@ -751,7 +791,7 @@ int zolo_polar(Context& c, int rk, int m, int n, const double* dA, int64_t lda, 
   }
   // bounds left the factored A/alpha in its workspace ("bnd_x", ld even(m)) and the panel factors in "bnd_t"
   const Prefactored pf{c.buf("bnd_x", static_cast<size_t>(even(m)) * n), even(m),
-                       c.buf("bnd_t", static_cast<size_t>(npanels(n)) * 1024)};
+                       c.buf("bnd_t", static_cast<size_t>(npanels(n)) * 1024), alpha_fro};
   const int info = zolo_pd(c, 'N', rk, m, n, alpha, beta, dA, lda, dQ, ldq, dH, ldh, 6, &pf);
   c.stats.ms_bounds = ms_bounds;
   c.stats.flops += bflops;

@@ -11,11 +11,15 @@ enum BoundsMode {
   BOUNDS_PQDWHFACS = 0,  // beta = ||X0||_1 / (sqrt(n) ||R^-1||_1)   (pqdwhfacs.f90:325-344 form)
   BOUNDS_ZOLOPD = 1,     // beta = 1 / (sqrt(n) ||R^-1||_1)           (zolopd.f90 / test_zolodrv1.f90 form)
   BOUNDS_FROB = 2,       // beta = 1 / ||R^-1||_F: still <= sigma_min(X0), never below mode 1's
+  BOUNDS_NORM2 = 3,      // mode 2's beta, and alpha lowered from ||A||_F to a guaranteed upper bound of
+                         // ||A||_2, (sum_i sigma_i^16)^(1/16) from (R^T R)^4 (norm2_upper in polar.cpp)
 };
 
 // alpha = ||A - sigma I||_F ; beta from R of (A - sigma I)/alpha = QR.  Returns info (0 ok).
+// BOUNDS_NORM2: alpha is then the two-norm bound and beta the sigma_min bound of A/alpha; the
+// QR left in the workspace is that of A/alpha_fro (reported in *alpha_fro when not null).
 int bounds(Context& c, int m, int n, double sigma, const double* dA, int64_t lda, BoundsMode mode, double* alpha,
-           double* beta);
+           double* beta, double* alpha_fro = nullptr);
 
 struct QdwhOpts {
   char sym = 'N';
@@ -35,6 +39,7 @@ struct Prefactored {
   const double* W;
   int64_t ldw;
   const double* T;
+  double alpha;  // the factored matrix is A / alpha
 };
 
 // Zolo-PD of As/(alpha*beta) with rk terms (pzolopd1.f90:280-487); H as above.  With
