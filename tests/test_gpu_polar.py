@@ -491,7 +491,7 @@ def _run_polar(h, a, m, n, fast, inject=0, qdwh=False):
     elif fast:
         info = zb.polar_dev(h, 8, m, n, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n)
     else:
-        al, be, _ = zo.bounds_zolodrv(a)
+        al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)  # the driver's estimate, QR form
         info = zb.pzolopd1_dev(h, "N", 8, m, n, al, be, da.data_ptr(), m, dq.data_ptr(), m, dh.data_ptr(), n)
     h.set_option(zb.OPT_INJECT_CHOL_FAIL, 0)
     return info, zb.device_to_colmajor(dq), zb.device_to_colmajor(dh), h.stats()
