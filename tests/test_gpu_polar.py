@@ -364,7 +364,7 @@ def test_bounds_frobenius_mode(m, n, kappa):
     assert abs(be2 - ref) <= max(1e-10, 100 * n * EPS * kappa) * ref
     assert be1 * (1 - 1e-8) <= be2 <= s[-1] / al * (1 + 1e-8)
     with pytest.raises(zb.ZoloError):
-        zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=3)
+        zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=4)
     h.close()
 
 
@@ -537,7 +537,9 @@ def test_matrixmarket_symmetric_through_pqdwhfacs(tmp_path):
     q, h, info = zb.pqdwhfacs("S", dense, sigma=sigma, polar="T")
     assert info == 0
     shifted = dense - sigma * np.eye(n)
-    check_pd(shifted, q, h, n)
+    # H = sym(Q^T A) of the unshifted A (pqdwhfacs.f90:460-464), so the polar factor of A - sigma I
+    # is Q with H - sigma sym(Q)
+    check_pd(shifted, q, h - sigma * 0.5 * (q + q.T), n)
     q_o, h_o, st_o = zo.pqdwhfacs("S", dense, sigma=sigma, polar="T")
     ev = np.abs(np.linalg.eigvalsh(shifted))
     kappa = ev.max() / ev.min()

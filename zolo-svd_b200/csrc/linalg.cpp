@@ -18,6 +18,37 @@ int split_point(int n) {
   if (n1 <= 0) n1 = n / 2;
   return n1;
 }
+// Algorithmic flops of a product: lower triangle only (tri); k >= output column (kfrom_n); the
+// triangular operand's zero k range skipped (kfrom_n / kto_m).
+double algo_flops(int M, int N, int K, int tri, int kfrom_n, int kto_m) {
+  double f = (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K;
+  if (kfrom_n == 2) {
+    // row i uses k >= i, over its lower-triangle (tri) or all N columns
+    f = 0.0;
+    for (int i = 0; i < std::min(M, K); ++i) f += 2.0 * (tri ? std::min(i + 1, N) : N) * (K - i);
+  } else if (kfrom_n == 3) {
+    // entry (i, j) uses k >= max(i, j) (no tri)
+    f = 0.0;
+    for (int i = 0; i < std::min(M, K); ++i) {
+      const double jn = std::min(i + 1, N);  // columns j <= i: K - i each
+      const double jm = std::max(0, std::min(N, K) - i - 1);  // columns i < j < K: K - j each
+      f += 2.0 * (jn * (K - i) + jm * (K - i - 1) - jm * (jm - 1.0) / 2.0);
+    }
+  } else if (kfrom_n) {
+    const double nn = std::min(N, K);
+    f = 2.0 * M * (static_cast<double>(N) * K - nn * (nn - 1.0) / 2.0 - (N - nn) * static_cast<double>(K));
+  }
+  if (kto_m == 2) {
+    // column j uses k <= j: sum over columns of min(K, j + 1)
+    const double nn = std::min(N, K);
+    f = 2.0 * M * (nn * (nn + 1.0) / 2.0 + (N - nn) * static_cast<double>(K));
+  } else if (kto_m) {
+    // row i uses k <= i: sum over rows of min(K, i + 1)
+    const double mm = std::min(M, K);
+    f = 2.0 * N * (mm * (mm + 1.0) / 2.0 + (M - mm) * static_cast<double>(K));
+  }
+  return f;
+}
 }  // namespace
 
 namespace {
@@ -71,33 +102,7 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   Profiler::Rec rec;
   const int cls = tri ? 6 : (M <= 32 ? 3 : (N <= 64 ? 4 : (K <= 64 ? 5 : 0)));
   if (c.prof.on) {
-    // algorithmic flops: lower triangle only (tri); k >= output column (kfrom_n)
-    double f = (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K;
-    if (kfrom_n == 2) {
-      // row i uses k >= i, over its lower-triangle (tri) or all N columns
-      f = 0.0;
-      for (int i = 0; i < std::min(M, K); ++i) f += 2.0 * (tri ? std::min(i + 1, N) : N) * (K - i);
-    } else if (kfrom_n == 3) {
-      // entry (i, j) uses k >= max(i, j) (no tri)
-      f = 0.0;
-      for (int i = 0; i < std::min(M, K); ++i) {
-        const double jn = std::min(i + 1, N);  // columns j <= i: K - i each
-        const double jm = std::max(0, std::min(N, K) - i - 1);  // columns i < j < K: K - j each
-        f += 2.0 * (jn * (K - i) + jm * (K - i - 1) - jm * (jm - 1.0) / 2.0);
-      }
-    } else if (kfrom_n) {
-      const double nn = std::min(N, K);
-      f = 2.0 * M * (static_cast<double>(N) * K - nn * (nn - 1.0) / 2.0 - (N - nn) * static_cast<double>(K));
-    }
-    if (kto_m == 2) {
-      // column j uses k <= j: sum over columns of min(K, j + 1)
-      const double nn = std::min(N, K);
-      f = 2.0 * M * (nn * (nn + 1.0) / 2.0 + (N - nn) * static_cast<double>(K));
-    } else if (kto_m) {
-      // row i uses k <= i: sum over rows of min(K, i + 1)
-      const double mm = std::min(M, K);
-      f = 2.0 * N * (mm * (mm + 1.0) / 2.0 + (M - mm) * static_cast<double>(K));
-    }
+    const double f = algo_flops(M, N, K, tri, kfrom_n, kto_m);
     c.prof.begin(cls, f * batch, s, &rec);
   }
   ck(dgemm(a, c.splitk(side), s));
@@ -157,7 +162,7 @@ void ozgemm(Context& c, int transA, int transB, int M, int N, int K, double alph
   w.status = c.oz_status_word();
   Profiler::Rec rec;
   if (c.prof.on) {
-    const double f = (tri ? 1.0 : 2.0) * M * static_cast<double>(N) * K;
+    const double f = algo_flops(M, N, K, tri, kfrom_n, kto_m);
     c.prof.begin(7, f * batch, s, &rec);
   }
   ck(zolo::ozgemm(a, slices, w, s, num_sms()));
