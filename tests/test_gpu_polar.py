@@ -597,3 +597,29 @@ def test_norm2_upper_bound_on_config_spectra(cfg):
     h.close()
     if cons[0] is not None:
         assert cons[1] <= cons[0] * (1 + 1e-12)
+
+
+def test_sharded_driver_device_backend_matches_pzolopd1():
+    """The r-term sharded driver (sharded.py) on one GPU with the library's per-term kernels
+    (one rank, so no all-reduce): the reference's iteration, the same branch sequence and
+    polar factor as zolo_pzolopd1_dev with per-term stacked QRs."""
+    import importlib
+    import torch
+    sh = importlib.import_module("zolo_svd_b200.sharded")
+    m, n, kappa = 260, 200, 1e10
+    a, u, v = zo.make_matrix(n, np.geomspace(1.0, 1.0 / kappa, n), 777, m=m)
+    h = zb.Handle(0)
+    h.set_option(zb.OPT_SHARED_QR, 0)
+    da = zb.colmajor_to_device(a)
+    torch.cuda.synchronize()
+    al, be, _ = zb.bounds_dev(h, m, n, da.data_ptr(), m, mode=1)
+    dq = torch.zeros_like(da)
+    assert zb.pzolopd1_dev(h, "N", 8, m, n, al, be, da.data_ptr(), m, dq.data_ptr(), m) == 0
+    st = h.stats()
+    x = da.clone()
+    it, branches, info = sh.pzolopd1_sharded("N", 8, m, n, al, be, x, sh.DeviceBackend(h))
+    h.close()
+    assert info == 0 and it == st["iterations"] and branches == st["branches"]
+    q1, q2 = zb.device_to_colmajor(dq), zb.device_to_colmajor(x)
+    assert np.linalg.norm(q1 - q2) / math.sqrt(n) <= 100 * n * EPS * kappa
+    assert zo.orthogonality(q2) <= tol_n(n)
