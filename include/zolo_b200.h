@@ -83,9 +83,10 @@ const char* zolo_version(void);
 /* Per-kernel-class device timing with CUDA events on the launching streams
  * (0 = DMMA GEMM general shapes, 1 = Householder panel, 2 = Cholesky leaf,
  * 3 = GEMM M <= 32, 4 = GEMM N <= 64, 5 = GEMM rank-k K <= 64, 6 = GEMM lower
- * triangle, 7 = FP64 product emulated on the INT8 tensor cores).  While enabled,
- * zolo_profile_read fills out[3*cls + 0..2] = {launches, milliseconds, algorithmic
- * flops} accumulated since the last reset (out holds 24 doubles). */
+ * triangle, 7 = FP64 product emulated on the INT8 tensor cores, 8 = GEMM with
+ * 64 < K <= 256, class 0 then being K > 256).  While enabled, zolo_profile_read fills
+ * out[3*cls + 0..2] = {launches, milliseconds, algorithmic flops} accumulated since the
+ * last reset (out holds 27 doubles). */
 int zolo_profile_enable(zolo_handle_t handle, int on);
 /* Thread-block-cluster size the Householder panel kernel uses for an m x w panel on the
  * current device (negative when the rows do not fit in shared memory). */

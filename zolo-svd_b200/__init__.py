@@ -161,7 +161,7 @@ OPT_OWN_BOUNDS = 8
 OPT_INJECT_CHOL_FAIL = 9
 OPT_NORM2_BOUND = 10
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
-                   "ozgemm"]
+                   "ozgemm", "dgemm_k256"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
 

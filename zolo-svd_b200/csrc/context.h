@@ -39,9 +39,10 @@ struct Stats {
 // their own stream: 0 = DMMA GEMM (general shapes, K > 64), 1 = Householder panel,
 // 2 = Cholesky leaf, 3 = GEMM with M <= 32, 4 = GEMM with N <= 64,
 // 5 = GEMM rank-k update (K <= 64), 6 = GEMM lower-triangle output, 7 = FP64 product
-// emulated on the INT8 tensor cores (ozgemm).
+// emulated on the INT8 tensor cores (ozgemm), 8 = GEMM with 64 < K <= 256 (the Householder
+// block-reflector updates); class 0 is then K > 256.
 struct Profiler {
-  static constexpr int kClasses = 8;
+  static constexpr int kClasses = 9;
   bool on = false;
   struct Rec {
     cudaEvent_t a, b;

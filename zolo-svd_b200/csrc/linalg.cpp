@@ -100,7 +100,7 @@ void gemm(Context& c, int transA, int transB, int M, int N, int K, double alpha,
   const bool side = s == c.side_stream() && s != c.stream();
   if (need) c.ensure_splitk(need, side);
   Profiler::Rec rec;
-  const int cls = tri ? 6 : (M <= 32 ? 3 : (N <= 64 ? 4 : (K <= 64 ? 5 : 0)));
+  const int cls = tri ? 6 : (M <= 32 ? 3 : (N <= 64 ? 4 : (K <= 64 ? 5 : (K <= 256 ? 8 : 0))));
   if (c.prof.on) {
     const double f = algo_flops(M, N, K, tri, kfrom_n, kto_m);
     c.prof.begin(cls, f * batch, s, &rec);
