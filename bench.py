@@ -166,6 +166,29 @@ def fp64_peak_tflops(torch) -> float:
     return best
 
 
+def int8_library_tops(torch) -> float:
+    """cuBLASLt INT8 GEMM (torch._int_mm, int32 out) 8192^3 throughput measured in this run: a
+    library INT8 rate beside the tensor peak the INT8-emulated GEMM is compared with."""
+    n = 8192
+    a = torch.randint(-127, 128, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-127, 128, (n, n), dtype=torch.int8, device="cuda").t().contiguous().t()
+    for _ in range(2):
+        torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
 # ---------------------------------------------------------------------------
 # CPU reference arm: the oracle restatement, one full solve of the same matrix
 # ---------------------------------------------------------------------------
@@ -338,8 +361,9 @@ def haar_np(rng, m: int, n: int):
 def bench_batch_c4(torch, zb, h, reps: int = 3) -> dict:
     """Configuration 4: 512 matrices, n log-uniform in [64, 1024], m = n (1 + U[0,1]), kappa
     log-uniform in [1e2, 1e14], s geometric; PCG64 seed 1004 (sizes, kappa) and 1004 + i
-    (member i's Haar factors).  One zolo_qdwh_batch_dev call per timed repetition; the worst
-    member's backward error and orthogonality over 10 n eps."""
+    (member i's Haar factors).  One zolo_qdwh_batch_dev call per timed repetition (cached bucket
+    graphs replayed; the synchronized loop, the first eager call and the capturing call timed
+    beside it); the worst member's backward error and orthogonality over 10 n eps."""
     rng = np.random.default_rng(1004)
     mats = []
     for i in range(512):
@@ -356,15 +380,27 @@ def bench_batch_c4(torch, zb, h, reps: int = 3) -> dict:
     members = [(a.shape[0], a.shape[1], x.data_ptr(), a.shape[0], q.data_ptr(), a.shape[0], hh.data_ptr(),
                 a.shape[1]) for (a, _), x, q, hh in zip(mats, da, dq, dh)]
     stream = torch.cuda.current_stream()
-    zb.qdwh_batch_dev(h, members)  # warm-up: workspace of the worker streams
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        info, its = zb.qdwh_batch_dev(h, members)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
+
+    def timed(calls):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(calls):
+            r = zb.qdwh_batch_dev(h, members)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / calls, r
+    # the host-synchronized loop (ZOLO_OPT_BATCH_GRAPH = 0), after a call that sizes the workspace
+    h.set_option(zb.OPT_BATCH_GRAPH, 0)
+    zb.qdwh_batch_dev(h, members)
+    ms_sync, _ = timed(1)
+    # the scheduled form: the first call of each bucket shape issues its launches eagerly, the
+    # second captures them as one graph per bucket, later calls replay the graphs (timed)
+    h.set_option(zb.OPT_BATCH_GRAPH, 1)
+    ms_first, _ = timed(1)
+    ms_capture, _ = timed(1)
+    ms, (info, its) = timed(reps)
+    gst = zb.batch_stats(h)
     st = h.stats()
     worst_b = worst_o = worst_s = 0.0
     for (a, s), x, q, hh in zip(mats, da, dq, dh):
@@ -382,7 +418,10 @@ def bench_batch_c4(torch, zb, h, reps: int = 3) -> dict:
            "tflops_useful": st["flops"] / (ms * 1e-3) / 1e12,
            "tflops_executed": st["flops_executed"] / (ms * 1e-3) / 1e12,
            "worst_backward_error_over_10neps": worst_b, "worst_orthogonality_over_10neps": worst_o,
-           "worst_sv_err_rel_smax": worst_s}
+           "worst_sv_err_rel_smax": worst_s,
+           "launch": "one CUDA graph per bucket (iterations, H, unpacking) replayed on four worker streams; "
+                     "bounds eager", "buckets": gst["buckets"], "graph_replays": gst["graph_replays"],
+           "ms_first_call_eager": ms_first, "ms_capture_call": ms_capture, "ms_synchronized_loop": ms_sync}
     del da, dq, dh
     torch.cuda.empty_cache()
     return out
@@ -391,8 +430,10 @@ def bench_batch_c4(torch, zb, h, reps: int = 3) -> dict:
 def bench_svd_c5(torch, zb, h) -> dict:
     """Configuration 5: Zolo-SVD of a 16384 x 8192 matrix, kappa = 1e10: 70 % of s geometric in
     [1e-10, 1], 20 % exactly 1, 10 % in clusters of relative gap 1e-9; Gaussians from PCG64 seed
-    1005, their QR (Haar factors) on the GPU.  One zolo_svd_dev call (Zolo-PD r = 8, FP64 fast
-    form, then the spectral divide-and-conquer eigensolver on H)."""
+    1005, their QR (Haar factors) on the GPU.  One zolo_svd_dev call per form on the same matrix
+    (Zolo-PD r = 8, then the spectral divide-and-conquer eigensolver on H): the FP64 fast form,
+    and the mixed form beside it (the Cholesky iterations, finish and Q/H products of both the
+    Zolo-PD and the eigensolver's QDWH solves on the INT8-emulated GEMM)."""
     m, n = 16384, 8192
     rng = np.random.default_rng(1005)
     n70, n20 = int(0.7 * n), int(0.2 * n)
@@ -415,21 +456,27 @@ def bench_svd_c5(torch, zb, h) -> dict:
     ds = torch.empty(n, dtype=torch.float64, device="cuda")
     dv = torch.empty((n, n), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    zb.svd_dev(h, m, n, da.data_ptr(), m, du.data_ptr(), m, ds.data_ptr(), dv.data_ptr(), n, algo=1, rk=8)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    U, V = du.T, dv.T
     eye = torch.eye(n, dtype=torch.float64, device="cuda")
     out = {"workload": "Zolo-SVD 16384 x 8192, kappa 1e10, 20 % sigma = 1, clusters of gap 1e-9 (zolo_svd_dev, "
-                       "Zolo-PD r = 8 FP64 fast form + spectral divide-and-conquer)",
-           "s": e0.elapsed_time(e1) / 1e3,
-           "residual": float(torch.linalg.norm(a - (U * ds[None, :]) @ V.T) / torch.linalg.norm(a)),
-           "sv_err_rel_smax": float(torch.max(torch.abs(torch.sort(ds, descending=True).values - st)) / st[0]),
-           "orth_u": float(torch.linalg.norm(U.T @ U - eye) / math.sqrt(n)),
-           "orth_v": float(torch.linalg.norm(V.T @ V - eye) / math.sqrt(n))}
+                       "Zolo-PD r = 8 + spectral divide-and-conquer), FP64 fast form and mixed form"}
+    saved = h.get_option(zb.OPT_MIXED)
+    for form, mixed in (("fp64", 0), ("mixed", 1)):
+        h.set_option(zb.OPT_MIXED, mixed)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        zb.svd_dev(h, m, n, da.data_ptr(), m, du.data_ptr(), m, ds.data_ptr(), dv.data_ptr(), n, algo=1, rk=8)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        U, V = du.T, dv.T
+        out[form] = {"s": e0.elapsed_time(e1) / 1e3,
+                     "residual": float(torch.linalg.norm(a - (U * ds[None, :]) @ V.T) / torch.linalg.norm(a)),
+                     "sv_err_rel_smax": float(torch.max(torch.abs(torch.sort(ds, descending=True).values - st))
+                                              / st[0]),
+                     "orth_u": float(torch.linalg.norm(U.T @ U - eye) / math.sqrt(n)),
+                     "orth_v": float(torch.linalg.norm(V.T @ V - eye) / math.sqrt(n))}
+    h.set_option(zb.OPT_MIXED, saved)
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["s"] / out["mixed"]["s"]
     del a, da, du, dv, eye
     torch.cuda.empty_cache()
     return out
@@ -459,6 +506,10 @@ def run_gpu(args):
     h.set_stream(stream.cuda_stream)
 
     peak = fp64_peak_tflops(torch)
+    try:
+        i8_lib = int8_library_tops(torch)
+    except Exception:  # torch._int_mm unavailable: the line carries null
+        i8_lib = None
     a_host, s_host = make_input(n, args.kappa, 1003 + rank)
     dA = torch.from_numpy(a_host.T.copy()).to("cuda")  # column-major storage: dA[j, i] = A[i, j]
     s_true = torch.from_numpy(s_host).to("cuda")
@@ -658,7 +709,10 @@ def run_gpu(args):
                                 "fp64_equivalent_tflops": oz["flops"] / (oz["ms"] * 1e-3) / 1e12 if oz["ms"] else None,
                                 "share_of_step": oz["ms"] / prof_ms if prof_ms else None,
                                 "launches_per_step": oz["launches"],
-                                "int8_products_per_fp64_product": OZ_PRODUCTS},
+                                "int8_products_per_fp64_product": OZ_PRODUCTS,
+                                "library_int8_tops": i8_lib,
+                                "library_int8_source": "cuBLASLt INT8 GEMM 8192^3 (torch._int_mm) measured in "
+                                                       "this run"},
             "kernel_classes": per_class,
             "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
                     "call": "pzolopd1_ (gfortran symbol) on pinned host arrays, default handle with ZOLO_FAST=1 "

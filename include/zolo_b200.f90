@@ -20,7 +20,8 @@ module zolo_b200
   public :: zolo_default_handle, zolo_create, zolo_destroy, zolo_set_option, zolo_release_workspace
   public :: zolo_polar_dev, zolo_pzolopd1_dev, zolo_qdwh_dev
   public :: ZOLO_OPT_SHARED_QR, ZOLO_OPT_NS_FINISH, ZOLO_OPT_CHOL_INVERSE, ZOLO_OPT_BETA_FROB, &
-            ZOLO_OPT_TERM_PLAN, ZOLO_OPT_MIXED, ZOLO_OPT_MIXED_SLICES, ZOLO_OPT_OWN_BOUNDS
+            ZOLO_OPT_TERM_PLAN, ZOLO_OPT_MIXED, ZOLO_OPT_MIXED_SLICES, ZOLO_OPT_OWN_BOUNDS, &
+            ZOLO_OPT_NORM2_BOUND, ZOLO_OPT_BATCH_GRAPH
 
   ! zolo_set_option options (values as in include/zolo_b200.h)
   integer(c_int), parameter :: ZOLO_OPT_SHARED_QR = 1
@@ -31,6 +32,8 @@ module zolo_b200
   integer(c_int), parameter :: ZOLO_OPT_MIXED = 6
   integer(c_int), parameter :: ZOLO_OPT_MIXED_SLICES = 7
   integer(c_int), parameter :: ZOLO_OPT_OWN_BOUNDS = 8
+  integer(c_int), parameter :: ZOLO_OPT_NORM2_BOUND = 10
+  integer(c_int), parameter :: ZOLO_OPT_BATCH_GRAPH = 11
 
   interface
     ! PZOLOPD1 (pzolopd1.f90:2): Zolo-PD of As/(ALPHA*BETA) with RK <= 8 terms; Q = polar factor.

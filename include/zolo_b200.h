@@ -172,6 +172,26 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * 7n^3/3 extra flops.  The intent of the reference's pdnormest (pdnormest.f90:44-79, a power
  * iteration for ||A||_2).  No reference counterpart as an option. */
 #define ZOLO_OPT_NORM2_BOUND 10
+/* ZOLO_OPT_BATCH_GRAPH: 1 (default) = zolo_qdwh_batch_dev computes each bucket's iteration
+ * schedule on the host from the members' bounds (L_k of a member follows from L_0 alone:
+ * the form of every step and its weights) and runs the iterations, H and the unpacking
+ * without a host synchronization per step, as one CUDA graph launch: captured the second
+ * time a bucket of the same shape and schedule is solved on the handle, replayed afterwards
+ * (the first time issues the same launches eagerly and sizes the workspace).  The stopping
+ * rule stays PQDWHFACS's (pqdwhfacs.f90:359): a member whose L has converged takes one more
+ * step only while its last error is above TOL1^(1/3), which a gate kernel decides on the
+ * device from the error just measured; a bucket's final step when it is such a step for all
+ * of its members runs only if one of them takes it (one read-back).  Every step's Cholesky
+ * INFO and error are read back at the end: a failed Cholesky step reruns the bucket through
+ * the synchronized loop (which takes the QR form there), and a member whose error is still
+ * above TOL1^(1/3) continues in that loop, so the result is the loop's.  2 = the same
+ * schedule, its launches always issued eagerly (no graph).  0 = the host-synchronized loop
+ * (pqdwhfacs.f90:359-457 per member, two synchronizations per step). */
+#define ZOLO_OPT_BATCH_GRAPH 11
+/* ZOLO_OPT_INJECT_BATCH_ERR (diagnostic, 0 = off): 1 = the batched solver's check after a
+ * scheduled run sees the first member of each bucket with its last error above TOL1^(1/3), so
+ * that member continues in the synchronized loop.  Host-side only. */
+#define ZOLO_OPT_INJECT_BATCH_ERR 12
 /* The default handle (used by the reference-named host-array entry points) reads its options
  * from the environment when it is created, so an unchanged Fortran driver selects them:
  * ZOLO_FAST=1 sets ZOLO_OPT_SHARED_QR, _NS_FINISH, _CHOL_INVERSE, _BETA_FROB, _TERM_PLAN and
@@ -288,6 +308,13 @@ int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, 
  * number of buckets and fills bucket[i] (member i's bucket), mb[], nb[] (per bucket, count
  * entries suffice) and the predicted ms; model NULL = the defaults; mode 1 = the fixed size
  * ladder instead of the optimized split. */
+/* Record of the handle's last zolo_qdwh_batch_dev call: out[0..11] = buckets, largest
+ * iteration count, executed FP64 flops (padding included), useful flops (unpadded sizes),
+ * device ms, the plan's predicted ms, and the buckets whose iterations ran as a cached graph
+ * replayed, a graph captured and launched, the schedule issued eagerly, the synchronized
+ * loop, a rerun after a failed Cholesky step, a continuation in the synchronized loop
+ * (ZOLO_OPT_BATCH_GRAPH).  Returns 0. */
+int zolo_batch_stats(zolo_handle_t h, double* out);
 int zolo_batch_autotune(zolo_handle_t h, double* model);
 int zolo_batch_set_model(zolo_handle_t h, const double* model);
 int zolo_batch_plan(int count, const int* m, const int* n, const double* model, int max_batch, int mode,

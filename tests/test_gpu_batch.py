@@ -88,6 +88,75 @@ def test_batch_bad_member_and_empty():
     h.close()
 
 
+def _close(xs, ys, rel):
+    for x, y in zip(xs, ys):
+        assert np.max(np.abs(x - y)) <= rel * max(1.0, np.max(np.abs(y)))
+
+
+def test_batch_graph_matches_synchronized_loop():
+    """ZOLO_OPT_BATCH_GRAPH: the scheduled run (issued eagerly on the first call of a bucket
+    shape, captured as a graph on the second, the cached graph replayed on the third; or
+    always eagerly with option value 2) takes the synchronized loop's steps: the same
+    iteration counts and, to rounding, the same Q and H."""
+    h = zb.Handle(0)
+    mats = _members(3, 24, 5, 300)
+    h.set_option(zb.OPT_BATCH_GRAPH, 0)
+    info0, its0, q0, h0 = _run_batch(h, mats)
+    st = zb.batch_stats(h)
+    assert st["buckets"] > 1 and st["sync_loops"] == st["buckets"]
+    h.set_option(zb.OPT_BATCH_GRAPH, 1)
+    for call, key in enumerate(("eager_scheduled", "graph_captures", "graph_replays")):
+        info, its, q, hh = _run_batch(h, mats)
+        st = zb.batch_stats(h)
+        assert st[key] == st["buckets"], (call, st)
+        assert st["restarts"] == 0 and st["resumes"] == 0 and st["sync_loops"] == 0
+        assert info == info0 and its == its0
+        _close(q, q0, 1e-13)
+        _close(hh, h0, 1e-13)
+    h.set_option(zb.OPT_BATCH_GRAPH, 2)  # the schedule issued eagerly on every call
+    info, its, q, hh = _run_batch(h, mats)
+    st = zb.batch_stats(h)
+    assert st["eager_scheduled"] == st["buckets"] and st["graph_replays"] == 0
+    assert info == info0 and its == its0
+    _close(q, q0, 1e-13)
+    h.close()
+
+
+@pytest.mark.parametrize("inject", ["cholesky", "error"])
+def test_batch_graph_recovery_paths(inject):
+    """The checks after a scheduled run, driven by host-side injection: a Cholesky step
+    reported failed reruns its bucket through the synchronized loop (QR form at that step);
+    a member whose last error is reported high continues there for one more step.  Both on
+    the eager and on the captured run; every member stays accurate."""
+    h = zb.Handle(0)
+    mats = _members(4, 16, 20, 200)
+    info0, its0, _, _ = _run_batch(h, mats)
+    h.release()
+    if inject == "cholesky":
+        h.set_option(zb.OPT_INJECT_CHOL_FAIL, 4)  # the fourth step, a Cholesky-form one
+    else:
+        h.set_option(zb.OPT_INJECT_BATCH_ERR, 1)
+    for call in range(2):
+        info, its, qs, hs = _run_batch(h, mats)
+        st = zb.batch_stats(h)
+        assert st["eager_scheduled" if call == 0 else "graph_captures"] == st["buckets"]
+        assert info == [0] * len(mats)
+        if inject == "cholesky":
+            assert st["restarts"] >= 1 and st["resumes"] == 0
+        else:
+            assert st["resumes"] == st["buckets"] and st["restarts"] == 0
+            d = [b - a for a, b in zip(its0, its)]
+            assert set(d) <= {0, 1} and sum(d) == st["buckets"], d
+        for (a, uv, s, kappa), q, hh in zip(mats, qs, hs):
+            n = a.shape[1]
+            assert zo.backward_error(a, q, hh) <= tol_n(n)
+            assert zo.orthogonality(q) <= tol_n(n)
+            assert np.linalg.norm(q - uv) / math.sqrt(n) <= max(1e-12, 100 * n * EPS * kappa)
+    h.set_option(zb.OPT_INJECT_CHOL_FAIL, 0)
+    h.set_option(zb.OPT_INJECT_BATCH_ERR, 0)
+    h.close()
+
+
 def config4_members(seed=1004, count=512):
     """Configuration 4: n = round(exp U[ln 64, ln 1024]), m = round(n (1 + U[0, 1])),
     kappa = 10^U[2, 14], s geometric from 1 to 1/kappa; member i generated from PCG64 seed
@@ -105,7 +174,8 @@ def config4_members(seed=1004, count=512):
 
 
 def test_batch_config4_full_size():
-    """The 512-member configuration at full size in one call: every member backward stable and
+    """The 512-member configuration at full size in one call (run three times: eagerly, captured,
+    replayed, with the same results): every member backward stable and
     orthogonal to 10 n eps, its singular values within 1e-12 sigma_max, its polar factor within
     100 n eps kappa of U V^T; a sample of members against the oracle's PQDWHFACS."""
     import torch
@@ -117,8 +187,20 @@ def test_batch_config4_full_size():
     torch.cuda.synchronize()
     members = [(a.shape[0], a.shape[1], d.data_ptr(), a.shape[0], q.data_ptr(), a.shape[0], hh.data_ptr(),
                 a.shape[1]) for (a, *_), d, q, hh in zip(mats, dev, dq, dh)]
-    info, its = zb.qdwh_batch_dev(h, members)
-    assert info == [0] * len(mats)
+    # three calls: the schedule issued eagerly, captured as graphs, the graphs replayed
+    first = None
+    for key in ("eager_scheduled", "graph_captures", "graph_replays"):
+        for q in dq:
+            q.zero_()
+        info, its = zb.qdwh_batch_dev(h, members)
+        st = zb.batch_stats(h)
+        assert st[key] == st["buckets"] and st["restarts"] == 0, st
+        assert info == [0] * len(mats)
+        if first is None:
+            first = ([q.clone() for q in dq], its)
+        else:
+            assert its == first[1]
+            assert max(float(torch.max(torch.abs(q - q1))) for q, q1 in zip(dq, first[0])) <= 1e-13
     worst = 0.0
     for k, ((a, u, v, s, kappa), q_d, h_d) in enumerate(zip(mats, dq, dh)):
         m, n = a.shape

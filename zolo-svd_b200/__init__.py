@@ -122,6 +122,7 @@ _SIGS = [
                                   C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_int64,
                                   C.c_int, C.c_int, C.c_int]),
     ("zolo_batch_autotune", C.c_int, [C.c_void_p, c_double_p]),
+    ("zolo_batch_stats", C.c_int, [C.c_void_p, c_double_p]),
     ("zolo_batch_set_model", C.c_int, [C.c_void_p, c_double_p]),
     ("zolo_batch_plan", C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p,
                                   c_int_p, c_double_p]),
@@ -160,6 +161,8 @@ OPT_MIXED_SLICES = 7
 OPT_OWN_BOUNDS = 8
 OPT_INJECT_CHOL_FAIL = 9
 OPT_NORM2_BOUND = 10
+OPT_BATCH_GRAPH = 11
+OPT_INJECT_BATCH_ERR = 12
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
                    "ozgemm", "dgemm_k256"]
 
@@ -494,6 +497,18 @@ def qdwh_batch_dev(h: Handle, members, with_h: bool = True):
     its = (C.c_int * k)()
     _ck("zolo_qdwh_batch_dev", lib().zolo_qdwh_batch_dev(h.ptr, k, m, n, a, lda, q, ldq, hh, ldh, info, its))
     return list(info), list(its)
+
+
+BATCH_STATS_KEYS = ("buckets", "max_iterations", "flops", "flops_useful", "ms", "predicted_ms", "graph_replays",
+                    "graph_captures", "eager_scheduled", "sync_loops", "restarts", "resumes")
+
+
+def batch_stats(h: Handle) -> dict:
+    """Record of the handle's last qdwh_batch_dev call (zolo_batch_stats)."""
+    out = (C.c_double * 12)()
+    _ck("zolo_batch_stats", lib().zolo_batch_stats(h.ptr, out))
+    return {k: (int(v) if k not in ("flops", "flops_useful", "ms", "predicted_ms") else float(v))
+            for k, v in zip(BATCH_STATS_KEYS, out)}
 
 
 def polar_dev(h: Handle, rk: int, m: int, n: int, dA: int, lda: int, dQ: int, ldq: int, dH: int = 0,

@@ -149,6 +149,21 @@ __global__ void combine_batch_kernel(int m, int n, double* X, int64_t ldx, int64
   if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
+// A member whose step in this row is conditional (cond[b] != 0) takes it only when the previous
+// step's error sqrt(err2_prev[b]) is above tol; otherwise its coefficients become neutral
+// (Cholesky form: c = 0, so that the shifted Gram is I; QR form: scale 1; cx = 1, cz = 0,
+// which leaves X_b unchanged and its error 0).
+__global__ void gate_batch_kernel(int batch, const double* err2_prev, const double* cond, double* row, int qr,
+                                  double tol) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  if (cond[b] != 0.0 && !(sqrt(err2_prev[b]) > tol)) {
+    row[b] = qr ? 1.0 : 0.0;
+    row[batch + b] = 1.0;
+    row[2 * batch + b] = 0.0;
+  }
+}
+
 // G_b += d I
 __global__ void add_diag_batch_kernel(int n, double* G, int64_t ldg, int64_t sg, double d) {
   double* Gb = G + blockIdx.y * sg;
@@ -239,6 +254,13 @@ cudaError_t batch_combine(int m, int n, double* X, int64_t ldx, int64_t sx, cons
   if (static_cast<int64_t>(nb) * batch > partial_cap) nb = std::max(1, partial_cap / batch);
   combine_batch_kernel<<<dim3(nb, batch), TPB, 0, st>>>(m, n, X, ldx, sx, Z, ldz, sz, cx, cz, partial);
   reduce_rows_kernel<<<batch, TPB, 0, st>>>(partial, nb, err2);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_gate(int batch, const double* err2_prev, const double* cond, double* row, int qr, double tol,
+                       cudaStream_t st) {
+  if (batch <= 0) return cudaSuccess;
+  gate_batch_kernel<<<(batch + TPB - 1) / TPB, TPB, 0, st>>>(batch, err2_prev, cond, row, qr, tol);
   return cudaGetLastError();
 }
 

@@ -21,6 +21,7 @@
 struct zolo_handle_s {
   explicit zolo_handle_s(int dev) : ctx(dev) {}
   zolo::Context ctx;
+  zolo::BatchStats last_batch;  // the last zolo_qdwh_batch_dev call
 };
 
 namespace {
@@ -134,6 +135,13 @@ int set_option(Context& c, int option, int value) {
     case ZOLO_OPT_NORM2_BOUND:
       c.zolo_norm2 = value != 0;
       return 0;
+    case ZOLO_OPT_BATCH_GRAPH:
+      if (value < 0 || value > 2) return -3;
+      c.batch_graph = value;
+      return 0;
+    case ZOLO_OPT_INJECT_BATCH_ERR:
+      c.inject_batch_err = value != 0;
+      return 0;
     default:
       return -1;
   }
@@ -164,7 +172,8 @@ void apply_env_options(Context& c) {
       {"ZOLO_OPT_SHARED_QR", ZOLO_OPT_SHARED_QR},   {"ZOLO_OPT_NS_FINISH", ZOLO_OPT_NS_FINISH},
       {"ZOLO_OPT_CHOL_INVERSE", ZOLO_OPT_CHOL_INVERSE}, {"ZOLO_OPT_BETA_FROB", ZOLO_OPT_BETA_FROB},
       {"ZOLO_OPT_TERM_PLAN", ZOLO_OPT_TERM_PLAN},   {"ZOLO_OPT_MIXED", ZOLO_OPT_MIXED},
-      {"ZOLO_OPT_MIXED_SLICES", ZOLO_OPT_MIXED_SLICES}, {"ZOLO_OPT_OWN_BOUNDS", ZOLO_OPT_OWN_BOUNDS}};
+      {"ZOLO_OPT_MIXED_SLICES", ZOLO_OPT_MIXED_SLICES}, {"ZOLO_OPT_OWN_BOUNDS", ZOLO_OPT_OWN_BOUNDS},
+      {"ZOLO_OPT_NORM2_BOUND", ZOLO_OPT_NORM2_BOUND},   {"ZOLO_OPT_BATCH_GRAPH", ZOLO_OPT_BATCH_GRAPH}};
   for (const auto& nm : names)
     if (get(nm.first, &v)) set_option(c, nm.second, v);
 }
@@ -331,6 +340,8 @@ int zolo_get_option(zolo_handle_t h, int option, int* value) {
       case ZOLO_OPT_OWN_BOUNDS: *value = c.zolo_own_bounds; return 0;
       case ZOLO_OPT_INJECT_CHOL_FAIL: *value = c.inject_chol_fail; return 0;
       case ZOLO_OPT_NORM2_BOUND: *value = c.zolo_norm2; return 0;
+      case ZOLO_OPT_BATCH_GRAPH: *value = c.batch_graph; return 0;
+      case ZOLO_OPT_INJECT_BATCH_ERR: *value = c.inject_batch_err; return 0;
       default: return -1;
     }
   });
@@ -484,8 +495,27 @@ int zolo_qdwh_batch_dev(zolo_handle_t h, int count, const int* m, const int* n, 
   if (count < 0) return -2;
   if (count > 0 && (!m || !n || !dA || !lda || !dQ || !ldq || !info || (dH && !ldh))) return -3;
   return guarded(h, [&](Context& c) {
-    return zolo::qdwh_batch(c, count, m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, nullptr);
+    zolo::BatchStats bs;
+    const int r = zolo::qdwh_batch(c, count, m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, &bs);
+    h->last_batch = bs;
+    return r;
   });
+}
+
+int zolo_batch_stats(zolo_handle_t h, double* out) {
+  if (!h) return -999;
+  if (!out) return -2;
+  std::lock_guard<std::mutex> lk(h->ctx.mu);
+  {
+    const zolo::BatchStats& b = h->last_batch;
+    const double v[12] = {static_cast<double>(b.buckets), static_cast<double>(b.max_iterations), b.flops,
+                          b.flops_useful, b.ms, b.predicted_ms, static_cast<double>(b.graph_replays),
+                          static_cast<double>(b.graph_captures), static_cast<double>(b.eager_scheduled),
+                          static_cast<double>(b.sync_loops), static_cast<double>(b.restarts),
+                          static_cast<double>(b.resumes)};
+    for (int i = 0; i < 12; ++i) out[i] = v[i];
+  }
+  return 0;
 }
 
 int zolo_batch_autotune(zolo_handle_t h, double* model) {

@@ -24,50 +24,73 @@ Context::~Context() {
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
+void Context::drop_graphs() {
+  for (auto& kv : graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  graphs.clear();
+}
+
+void Context::free_retired() {
+  for (void* p : retired_) cudaFree(p);
+  retired_.clear();
+}
+
 void Context::release_all() {
   workers.clear();
   if (stream_) cudaStreamSynchronize(stream_);
   if (side_) cudaStreamSynchronize(side_);
+  drop_graphs();
+  free_retired();
   for (auto& kv : bufs_) cudaFree(kv.second.first);
   bufs_.clear();
+  ++alloc_gen_;
   if (splitk_.ptr) cudaFree(splitk_.ptr);
   if (splitk_side_.ptr) cudaFree(splitk_side_.ptr);
   splitk_ = Scratch{};
   splitk_side_ = Scratch{};
 }
 
-static void* grow(std::map<std::string, std::pair<void*, size_t>>& bufs, const std::string& name, size_t bytes,
-                  cudaStream_t st) {
-  auto it = bufs.find(name);
-  if (it != bufs.end() && it->second.second >= bytes) return it->second.first;
-  if (it != bufs.end()) {
-    // kernels queued on the stream may still use the old block
-    ck(cudaStreamSynchronize(st));
-    ck(cudaFree(it->second.first));
-    bufs.erase(it);
+void* Context::grow(const std::string& name, size_t bytes) {
+  auto it = bufs_.find(name);
+  if (it != bufs_.end() && it->second.second >= bytes) return it->second.first;
+  if (it != bufs_.end()) {
+    if (capturing) {
+      retired_.push_back(it->second.first);  // captured nodes may reference the old block
+    } else {
+      // kernels queued on the stream may still use the old block
+      ck(cudaStreamSynchronize(stream_));
+      ck(cudaFree(it->second.first));
+    }
+    bufs_.erase(it);
+    ++alloc_gen_;
   }
   void* p = nullptr;
   const size_t b = bytes < 256 ? 256 : bytes;
   ck(cudaMalloc(&p, b));
-  bufs[name] = {p, b};
+  bufs_[name] = {p, b};
   return p;
 }
 
 double* Context::buf(const std::string& name, size_t elems) {
-  return static_cast<double*>(grow(bufs_, name, elems * sizeof(double), stream_));
+  return static_cast<double*>(grow(name, elems * sizeof(double)));
 }
 
 int* Context::ibuf(const std::string& name, size_t elems) {
-  return static_cast<int*>(grow(bufs_, name, elems * sizeof(int), stream_));
+  return static_cast<int*>(grow(name, elems * sizeof(int)));
 }
 
 void Context::ensure_splitk(size_t bytes, bool side) {
   Scratch& s = side ? splitk_side_ : splitk_;
   if (s.bytes >= bytes) return;
   if (s.ptr) {
-    ck(cudaStreamSynchronize(stream_));
-    ck(cudaStreamSynchronize(side_));
-    ck(cudaFree(s.ptr));
+    if (capturing) {
+      retired_.push_back(s.ptr);
+    } else {
+      ck(cudaStreamSynchronize(stream_));
+      ck(cudaStreamSynchronize(side_));
+      ck(cudaFree(s.ptr));
+    }
+    ++alloc_gen_;
   }
   s.ptr = nullptr;
   s.bytes = 0;

@@ -114,6 +114,13 @@ class Context {
   int zolo_norm2 = 0;
   // diagnostic: k + 1 = the Cholesky step of iteration k reports failure (0 = off)
   int inject_chol_fail = 0;
+  // diagnostic: 1 = the batched solver's scheduled run sees its first member's last error
+  // above the stopping tolerance (0 = off)
+  int inject_batch_err = 0;
+  // batched solver: 1 = each bucket's iterations, H and unpacking run as one CUDA graph
+  // launch from a host-computed schedule, 2 = the same launches issued eagerly, 0 = a
+  // host-synchronized loop
+  int batch_graph = 1;
   // batched solver: cost model of its bucket plan, and the worker contexts (own stream and
   // workspace each) its buckets run on concurrently
   BatchCostModel batch_model;
@@ -121,6 +128,23 @@ class Context {
   int oz_slices = 8;
   // digit planes of the products gemm() routes to ozgemm right now (0 = none); set by OzScope
   int oz_active = 0;
+
+  // Stream capture: while `capturing`, a buffer that must grow is replaced without a
+  // synchronization and the old block is kept alive (retired) until free_retired(), after
+  // the captured work has run.  alloc_gen changes whenever a block that captured work may
+  // reference is replaced or freed, which invalidates cached graphs.
+  bool capturing = false;
+  uint64_t alloc_gen() const { return alloc_gen_; }
+  void free_retired();
+  // cached executable graphs of the batched solver, by bucket shape and schedule
+  struct CachedGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t gen = 0;
+    int64_t launches = 0;
+    bool seen = false;  // the shape ran once eagerly (its workspace exists)
+  };
+  std::map<std::string, CachedGraph> graphs;
+  void drop_graphs();
 
   // small device scalars / partial sums
   double* dscal();     // 64 doubles
@@ -134,6 +158,9 @@ class Context {
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   std::map<std::string, std::pair<void*, size_t>> bufs_;
   Scratch splitk_, splitk_side_;
+  std::vector<void*> retired_;
+  uint64_t alloc_gen_ = 0;
+  void* grow(const std::string& name, size_t bytes);
 };
 
 // Routes the large products of gemm() to the INT8-emulated GEMM while in scope (when the

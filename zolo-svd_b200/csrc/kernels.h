@@ -202,6 +202,11 @@ cudaError_t batch_scale(int m, int n, double* X, int64_t ldx, int64_t sx, int ba
 cudaError_t batch_combine(int m, int n, double* X, int64_t ldx, int64_t sx, const double* Z, int64_t ldz, int64_t sz,
                           int batch, const double* cx, const double* cz, double* partial, int partial_cap,
                           double* err2, cudaStream_t st);
+// Conditional steps of the batched solver's schedule: where cond[b] != 0 and
+// sqrt(err2_prev[b]) <= tol, member b's coefficients in `row` (coef, cx, cz; batch entries
+// each) become neutral for the step's form (qr: 1, 1, 0; Cholesky: 0, 1, 0).
+cudaError_t batch_gate(int batch, const double* err2_prev, const double* cond, double* row, int qr, double tol,
+                       cudaStream_t st);
 cudaError_t batch_add_diag(int n, double* G, int64_t ldg, int64_t sg, int batch, double d, cudaStream_t st);
 cudaError_t batch_symmetrize(int n, double* B, int64_t ldb, int64_t sb, int batch, cudaStream_t st);
 cudaError_t batch_transpose(int m, int n, const double* A, int64_t lda, int64_t sa, double* B, int64_t ldb,

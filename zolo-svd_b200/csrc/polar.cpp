@@ -861,6 +861,7 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
     }
     hv[b] = done[b] ? 1.0 : 1.0 / alpha[b];
   }
+  const std::vector<double> xscale(hv.begin(), hv.begin() + B);  // X_0 = A' xscale
   h2d(c, vals, hv.data(), B);
   ck(scale_copy(MB, NB, 1.0, Ap, ldp, sP, X, ldp, sP, B, 0.0, st));
   ck(batch_scale(MB, NB, X, ldp, sP, B, vals, st));
@@ -918,98 +919,352 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
   int* dinfo = c.dinfo();
   std::vector<double> ak(B), bk(B), ckv(B), ln(B);
   std::vector<double> cx(B), cz(B);
-  int it = 0;
-  while (true) {
-    bool any = false, use_qr = false;
-    for (int b = 0; b < B; ++b) {
-      if (done[b]) continue;
-      any = true;
-      qdwh_weights(lowk[b], &ak[b], &bk[b], &ckv[b], &ln[b]);
-      use_qr = use_qr || ckv[b] > 100.0;
-    }
-    if (!any) break;
-    if (!use_qr) {
-      for (int b = 0; b < B; ++b) hv[b] = done[b] ? 0.0 : ckv[b];
-      h2d(c, vals, hv.data(), B);
-      gemm(c, 1, 0, NB, NB, MB, 1.0, Mat{X, ldp, sP}, Mat{X, ldp, sP}, 0.0, G, B, vals, 1, 0);
-      ck(batch_add_diag(NB, G.p, G.ld, G.stride, B, 1.0, st));
-      ck(cudaMemsetAsync(dinfo, 0, sizeof(int) * B, st));
-      c.stats.launches += 2;
-      potrf(c, NB, G, B, dinfo, Dg);
-      std::vector<int> pin(B, 0);
-      ck(cudaMemcpyAsync(pin.data(), dinfo, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
-      ck(cudaStreamSynchronize(st));
-      bool fail = false;
-      for (int b = 0; b < B; ++b) fail = fail || (!done[b] && pin[b] != 0);
-      if (fail) {
-        use_qr = true;  // not numerically SPD for some member: this step takes the QR form
-      } else {
-        spd_solve(c, MB, NB, X, ldp, G, Dg, Z, B, false, sP);
-        for (int b = 0; b < B; ++b) {
-          cx[b] = done[b] ? 1.0 : bk[b] / ckv[b];
-          cz[b] = done[b] ? 0.0 : ak[b] - bk[b] / ckv[b];
-        }
-        flops += B * (2.0 * MB * static_cast<double>(NB) * NB + NB * static_cast<double>(NB) * NB / 3.0 +
-                      static_cast<double>(MB) * NB * NB);
-        for (int b = 0; b < B; ++b) {
-          if (done[b]) continue;
-          const double mm = m[idx[b]], nn = n[idx[b]];
-          useful += 3.0 * mm * nn * nn + nn * nn * nn / 3.0;
-        }
-      }
-    }
-    if (use_qr) {
-      for (int b = 0; b < B; ++b) hv[b] = done[b] ? 1.0 : 1.0 / std::sqrt(ckv[b]);
-      h2d(c, vals, hv.data(), B);
-      ck(form_stack(MB, mp, NB, X, ldp, W.p, W.ld, W.stride, vals, 0.0, B, st, 0, sP));
-      c.stats.launches++;
-      geqrf(c, mp + NB, NB, mp, W, tau, T, B);
-      orgqr(c, mp + NB, NB, mp, W, T, Qf, B);
-      q1q2t(c, MB, mp, NB, Qf, Z, B);
-      for (int b = 0; b < B; ++b) {
-        const double sck = done[b] ? 1.0 : std::sqrt(ckv[b]);
-        cx[b] = done[b] ? 1.0 : bk[b] / ckv[b];
-        cz[b] = done[b] ? 0.0 : (ak[b] - bk[b] / ckv[b]) / sck;
-      }
-      flops += B * (4.0 * MB * static_cast<double>(NB) * NB + static_cast<double>(NB) * NB * NB);
-      for (int b = 0; b < B; ++b) {
-        if (done[b]) continue;
-        const double mm = m[idx[b]], nn = n[idx[b]];
-        useful += 4.0 * mm * nn * nn + nn * nn * nn;
-      }
-    }
-    for (int b = 0; b < B; ++b) {
-      hv[B + b] = cx[b];
-      hv[2 * B + b] = cz[b];
-    }
-    h2d(c, vals + B, hv.data() + B, 2 * B);
-    ck(batch_combine(MB, NB, X, ldp, sP, Z.p, Z.ld, Z.stride, B, vals + B, vals + 2 * B, part, 8192, vals + 3 * B,
-                     st));
+  const std::vector<char> done0 = done;
+  const std::vector<double> lowk0 = lowk;
+
+  // The steps on the device, their coefficients read from device arrays: the Cholesky form
+  // Z = X (I + c X^T X)^{-1} (pqdwhfacs.f90:408-431) and the QR form from the stack
+  // [sqrt(c) X; I] (pqdwhfacs.f90:375-404), then X <- cx X + cz Z and ||X_new - X||_F^2.
+  auto chol_factor = [&](const double* dck, int* dinf) {
+    gemm(c, 1, 0, NB, NB, MB, 1.0, Mat{X, ldp, sP}, Mat{X, ldp, sP}, 0.0, G, B, dck, 1, 0);
+    ck(batch_add_diag(NB, G.p, G.ld, G.stride, B, 1.0, st));
+    ck(cudaMemsetAsync(dinf, 0, sizeof(int) * B, st));
     c.stats.launches += 2;
-    const std::vector<double> e2 = d2h_vec(c, vals + 3 * B, B);
-    ++it;
-    for (int b = 0; b < B; ++b) {
-      if (done[b]) continue;
-      err[b] = std::sqrt(e2[b]);
-      lowk[b] = ln[b];
-      ++its[b];
-      // pqdwhfacs.f90:359: continue while ERR > TOL1^(1/3) or |1 - L| > TOL1, IT <= 12
-      const bool more = (err[b] > tol2 || std::fabs(1.0 - lowk[b]) > tol1) && its[b] <= maxit;
-      if (!more) done[b] = 1;
-    }
-  }
-  // ---- H' = sym(Q'^T A') and the unpadded outputs ----
-  double* Hp = nullptr;
-  if (dH) {
-    Hp = c.buf("bat_h", static_cast<size_t>(sN) * B);
-    gemm(c, 1, 0, NB, NB, MB, 1.0, Mat{X, ldp, sP}, Mat{Ap, ldp, sP}, 0.0, Mat{Hp, ldn, sN}, B);
-    ck(batch_symmetrize(NB, Hp, ldn, sN, B, st));
+    potrf(c, NB, G, B, dinf, Dg);
+  };
+  auto chol_solve = [&]() { spd_solve(c, MB, NB, X, ldp, G, Dg, Z, B, false, sP); };
+  auto qr_step = [&](const double* dsc) {
+    ck(form_stack(MB, mp, NB, X, ldp, W.p, W.ld, W.stride, dsc, 0.0, B, st, 0, sP));
     c.stats.launches++;
+    geqrf(c, mp + NB, NB, mp, W, tau, T, B);
+    orgqr(c, mp + NB, NB, mp, W, T, Qf, B);
+    q1q2t(c, MB, mp, NB, Qf, Z, B);
+  };
+  auto combine = [&](const double* dcx, const double* dcz, double* de2) {
+    ck(batch_combine(MB, NB, X, ldp, sP, Z.p, Z.ld, Z.stride, B, dcx, dcz, part, 8192, de2, st));
+    c.stats.launches += 2;
+  };
+  auto count_step = [&](bool qr, const std::vector<char>& active) {
+    flops += B * (qr ? 4.0 * MB * static_cast<double>(NB) * NB + static_cast<double>(NB) * NB * NB
+                     : 2.0 * MB * static_cast<double>(NB) * NB + NB * static_cast<double>(NB) * NB / 3.0 +
+                           static_cast<double>(MB) * NB * NB);
+    for (int b = 0; b < B; ++b) {
+      if (!active[b]) continue;
+      const double mm = m[idx[b]], nn = n[idx[b]];
+      useful += qr ? 4.0 * mm * nn * nn + nn * nn * nn : 3.0 * mm * nn * nn + nn * nn * nn / 3.0;
+    }
+  };
+  // H' = sym(Q'^T A') and the unpadded outputs
+  double* Hp = dH ? c.buf("bat_h", static_cast<size_t>(sN) * B) : nullptr;
+  auto finish = [&]() {
+    if (dH) {
+      gemm(c, 1, 0, NB, NB, MB, 1.0, Mat{X, ldp, sP}, Mat{Ap, ldp, sP}, 0.0, Mat{Hp, ldn, sN}, B);
+      ck(batch_symmetrize(NB, Hp, ldn, sN, B, st));
+      c.stats.launches++;
+    }
+    ck(batch_unpack(dmem, B, MB, NB, X, ldp, sP, Hp, ldn, sN, st));
+    c.stats.launches++;
+  };
+  auto count_finish = [&]() {
+    if (!dH) return;
     flops += B * 2.0 * MB * static_cast<double>(NB) * NB;
     for (int b = 0; b < B; ++b) useful += 2.0 * m[idx[b]] * static_cast<double>(n[idx[b]]) * n[idx[b]];
+  };
+
+  // The host-synchronized loop (pqdwhfacs.f90:359-457 per member): the weights and the form
+  // of each step from the members' current L, the Cholesky INFO read back before the solve (a
+  // factorization that fails for any member turns the step into the QR form) and the errors
+  // read back after the update.
+  int it = 0;
+  auto sync_loop = [&]() {
+    while (true) {
+      bool any = false, use_qr = false;
+      for (int b = 0; b < B; ++b) {
+        if (done[b]) continue;
+        any = true;
+        qdwh_weights(lowk[b], &ak[b], &bk[b], &ckv[b], &ln[b]);
+        use_qr = use_qr || ckv[b] > 100.0;
+      }
+      if (!any) break;
+      std::vector<char> active(B);
+      for (int b = 0; b < B; ++b) active[b] = !done[b];
+      if (!use_qr) {
+        for (int b = 0; b < B; ++b) hv[b] = done[b] ? 0.0 : ckv[b];
+        h2d(c, vals, hv.data(), B);
+        chol_factor(vals, dinfo);
+        std::vector<int> pin(B, 0);
+        ck(cudaMemcpyAsync(pin.data(), dinfo, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
+        ck(cudaStreamSynchronize(st));
+        bool fail = false;
+        for (int b = 0; b < B; ++b) fail = fail || (!done[b] && pin[b] != 0);
+        fail = fail || injected_info(c, it, 0) != 0;
+        if (fail) {
+          use_qr = true;  // not numerically SPD for some member: this step takes the QR form
+        } else {
+          chol_solve();
+          for (int b = 0; b < B; ++b) {
+            cx[b] = done[b] ? 1.0 : bk[b] / ckv[b];
+            cz[b] = done[b] ? 0.0 : ak[b] - bk[b] / ckv[b];
+          }
+          count_step(false, active);
+        }
+      }
+      if (use_qr) {
+        for (int b = 0; b < B; ++b) hv[b] = done[b] ? 1.0 : 1.0 / std::sqrt(ckv[b]);
+        h2d(c, vals, hv.data(), B);
+        qr_step(vals);
+        for (int b = 0; b < B; ++b) {
+          const double sck = done[b] ? 1.0 : std::sqrt(ckv[b]);
+          cx[b] = done[b] ? 1.0 : bk[b] / ckv[b];
+          cz[b] = done[b] ? 0.0 : (ak[b] - bk[b] / ckv[b]) / sck;
+        }
+        count_step(true, active);
+      }
+      for (int b = 0; b < B; ++b) {
+        hv[B + b] = cx[b];
+        hv[2 * B + b] = cz[b];
+      }
+      h2d(c, vals + B, hv.data() + B, 2 * B);
+      combine(vals + B, vals + 2 * B, vals + 3 * B);
+      const std::vector<double> e2 = d2h_vec(c, vals + 3 * B, B);
+      ++it;
+      for (int b = 0; b < B; ++b) {
+        if (done[b]) continue;
+        err[b] = std::sqrt(e2[b]);
+        lowk[b] = ln[b];
+        ++its[b];
+        // pqdwhfacs.f90:359: continue while ERR > TOL1^(1/3) or |1 - L| > TOL1, IT <= 12
+        const bool more = (err[b] > tol2 || std::fabs(1.0 - lowk[b]) > tol1) && its[b] <= maxit;
+        if (!more) done[b] = 1;
+      }
+    }
+  };
+
+  if (!c.batch_graph) {
+    sync_loop();
+    finish();
+    count_finish();
+    bs->sync_loops++;
+  } else {
+    // The schedule: L_k of every member follows from its L_0 alone (the weights of
+    // pqdwhfacs.f90:362-372), so the host computes every step's form and coefficients before
+    // the first one runs.  A member continues unconditionally while |1 - L| > TOL1 (and
+    // IT <= 12); once L has converged, the loop continues only while ERR > TOL1^(1/3), a value
+    // the device measures: that next step is scheduled as conditional, and a gate kernel
+    // makes it neutral for the member when the previous step's error is already below.
+    std::vector<char> act(B), sqr, pend(B, 0), hascond(B, 0);
+    for (int b = 0; b < B; ++b) act[b] = !done[b];
+    std::vector<double> l = lowk, lu = lowk, tab;
+    std::vector<int> cnt(B, 0), last(B, -1), kc(B, -1);
+    while (true) {
+      bool any = false, qr = false;
+      for (int b = 0; b < B; ++b) {
+        if (!act[b]) continue;
+        any = true;
+        qdwh_weights(l[b], &ak[b], &bk[b], &ckv[b], &ln[b]);
+        qr = qr || ckv[b] > 100.0;
+      }
+      if (!any) break;
+      const int k = static_cast<int>(sqr.size());
+      sqr.push_back(qr);
+      tab.resize(static_cast<size_t>(k + 1) * 5 * B, 0.0);
+      double* row = tab.data() + static_cast<size_t>(k) * 5 * B;
+      for (int b = 0; b < B; ++b) {
+        if (!act[b]) {
+          row[b] = qr ? 1.0 : 0.0;
+          row[B + b] = 1.0;
+          row[2 * B + b] = 0.0;
+          continue;
+        }
+        const double sck = std::sqrt(ckv[b]);
+        row[b] = qr ? 1.0 / sck : ckv[b];
+        row[B + b] = bk[b] / ckv[b];
+        row[2 * B + b] = qr ? (ak[b] - bk[b] / ckv[b]) / sck : ak[b] - bk[b] / ckv[b];
+        l[b] = ln[b];
+        if (pend[b]) {  // the conditional step: the member's last scheduled one
+          row[4 * B + b] = 1.0;
+          kc[b] = k;
+          hascond[b] = 1;
+          act[b] = 0;
+          continue;
+        }
+        ++cnt[b];
+        lu[b] = l[b];
+        last[b] = k;
+        if (cnt[b] > maxit) {
+          act[b] = 0;
+        } else if (!(std::fabs(1.0 - l[b]) > tol1)) {
+          pend[b] = 1;
+        }
+      }
+    }
+    const int K = static_cast<int>(sqr.size());
+    double* sched = c.buf("bat_sched", static_cast<size_t>(std::max(K, 1)) * 5 * B);
+    int* sinfo = c.ibuf("bat_sinfo", static_cast<size_t>(std::max(K, 1)) * B);
+    if (K > 0) h2d(c, sched, tab.data(), K * 5 * B);
+    std::vector<char> gated(K, 0);
+    for (int b = 0; b < B; ++b)
+      if (kc[b] >= 0) gated[kc[b]] = 1;
+    auto run_steps = [&](int k0, int k1) {
+      for (int k = k0; k < k1; ++k) {
+        double* row = sched + static_cast<size_t>(k) * 5 * B;
+        if (gated[k]) {
+          ck(batch_gate(B, row - 5 * B + 3 * B, row + 4 * B, row, sqr[k], tol2, st));
+          c.stats.launches++;
+        }
+        if (sqr[k]) {
+          qr_step(row);
+        } else {
+          chol_factor(row, sinfo + static_cast<size_t>(k) * B);
+          chol_solve();
+        }
+        combine(row + B, row + 2 * B, row + 3 * B);
+      }
+    };
+    // When the last step is conditional for every member in it, it runs only if one of them
+    // takes it (one read-back of the previous step's errors); the rest is one launch sequence.
+    bool tail = K > 0 && gated[K - 1];
+    for (int b = 0; b < B && tail; ++b) tail = last[b] < K - 1;
+    const int Ka = tail ? K - 1 : K;
+    auto scheduled = [&]() {
+      run_steps(0, Ka);
+      if (!tail) finish();
+    };
+    // one graph per bucket shape and schedule, captured on the second call of that shape (the
+    // first runs eagerly and sizes the workspace), replayed while the workspace is unchanged
+    std::string key = "qdwh " + std::to_string(MB) + " " + std::to_string(NB) + " " + std::to_string(B) + " " +
+                      (dH ? "h " : "- ") + (tail ? "t " : "- ");
+    for (int k = 0; k < Ka; ++k) key += sqr[k] ? (gated[k] ? 'Q' : 'q') : (gated[k] ? 'C' : 'c');
+    Context::CachedGraph& g = c.graphs[key];
+    cudaGraphExec_t once = nullptr;  // a graph captured while the workspace grew: run once
+    const bool capturable = c.batch_graph == 1 && !c.prof.on && st != cudaStreamLegacy && st != nullptr;
+    if (capturable && g.seen) {
+      if (g.exec && g.gen != c.alloc_gen()) {
+        ck(cudaGraphExecDestroy(g.exec));
+        g.exec = nullptr;
+      }
+      if (g.exec) {
+        ck(cudaGraphLaunch(g.exec, st));
+        c.stats.launches += g.launches;
+        bs->graph_replays++;
+      } else {
+        const uint64_t gen0 = c.alloc_gen();
+        const int64_t l0 = c.stats.launches;
+        cudaGraph_t graph = nullptr;
+        ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        c.capturing = true;
+        try {
+          scheduled();
+        } catch (...) {
+          c.capturing = false;
+          cudaStreamEndCapture(st, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        c.capturing = false;
+        ck(cudaStreamEndCapture(st, &graph));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        ck(e);
+        ck(cudaGraphLaunch(exec, st));
+        bs->graph_captures++;
+        if (c.alloc_gen() == gen0) {
+          g.exec = exec;
+          g.gen = gen0;
+          g.launches = c.stats.launches - l0;
+        } else {
+          once = exec;
+        }
+      }
+    } else {
+      scheduled();
+      g.seen = true;
+      bs->eager_scheduled++;
+    }
+    int Kr = K;  // steps that ran
+    if (tail) {
+      std::vector<double> e2p(B);
+      ck(cudaMemcpyAsync(e2p.data(), sched + static_cast<size_t>(K - 2) * 5 * B + 3 * B, sizeof(double) * B,
+                         cudaMemcpyDeviceToHost, st));
+      ck(cudaStreamSynchronize(st));
+      bool need = false;
+      for (int b = 0; b < B; ++b) need = need || (kc[b] == K - 1 && std::sqrt(e2p[b]) > tol2);
+      if (need) {
+        run_steps(K - 1, K);
+      } else {
+        Kr = K - 1;
+      }
+      finish();
+    }
+    // the last synchronization of the bucket's iterations: every step's INFO and error
+    std::vector<int> hinfo(static_cast<size_t>(K) * B, 0);
+    std::vector<double> hs(static_cast<size_t>(K) * 5 * B, 0.0);
+    if (K > 0) {
+      ck(cudaMemcpyAsync(hinfo.data(), sinfo, sizeof(int) * hinfo.size(), cudaMemcpyDeviceToHost, st));
+      ck(cudaMemcpyAsync(hs.data(), sched, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st));
+    }
+    ck(cudaStreamSynchronize(st));
+    if (once) ck(cudaGraphExecDestroy(once));
+    c.free_retired();
+    auto e2_at = [&](int k, int b) { return hs[static_cast<size_t>(k) * 5 * B + 3 * B + b]; };
+    // which members took their conditional step (the gate's test, repeated on the host)
+    std::vector<char> took(B, 0);
+    for (int b = 0; b < B; ++b) took[b] = hascond[b] && std::sqrt(e2_at(last[b], b)) > tol2;
+    for (int k = 0; k < Kr; ++k) {
+      std::vector<char> active(B, 0);
+      for (int b = 0; b < B; ++b) active[b] = (last[b] >= k) || (took[b] && kc[b] == k);
+      count_step(sqr[k], active);
+    }
+    count_finish();
+    bool fail = false;
+    for (int k = 0; k < Kr && !fail; ++k) {
+      if (sqr[k]) continue;
+      for (int b = 0; b < B; ++b) {
+        const bool active = (last[b] >= k) || (took[b] && kc[b] == k);
+        fail = fail || (active && hinfo[static_cast<size_t>(k) * B + b] != 0);
+      }
+      fail = fail || injected_info(c, k, 0) != 0;
+    }
+    if (fail) {
+      // a Cholesky step failed for some member: the whole bucket again from X_0 = A'/alpha
+      // through the synchronized loop, which takes the QR form at that step
+      h2d(c, vals, xscale.data(), B);
+      ck(scale_copy(MB, NB, 1.0, Ap, ldp, sP, X, ldp, sP, B, 0.0, st));
+      ck(batch_scale(MB, NB, X, ldp, sP, B, vals, st));
+      c.stats.launches += 2;
+      done = done0;
+      lowk = lowk0;
+      std::fill(its.begin(), its.end(), 0);
+      it = 0;
+      sync_loop();
+      finish();
+      count_finish();
+      bs->restarts++;
+    } else {
+      bool resume = false;
+      it = Kr;
+      for (int b = 0; b < B; ++b) {
+        if (last[b] < 0) continue;
+        const int kf = took[b] ? kc[b] : last[b];
+        its[b] = cnt[b] + (took[b] ? 1 : 0);
+        lowk[b] = took[b] ? l[b] : lu[b];
+        err[b] = std::sqrt(e2_at(kf, b));
+        // pqdwhfacs.f90:359 after the member's last step
+        const bool high = err[b] > tol2 || (c.inject_batch_err && b == 0);
+        done[b] = !((high || std::fabs(1.0 - lowk[b]) > tol1) && its[b] <= maxit);
+        resume = resume || !done[b];
+      }
+      if (resume) {
+        // a member whose error was still above TOL1^(1/3) after its conditional step: its
+        // further steps through the synchronized loop (the others are complete and unchanged)
+        sync_loop();
+        finish();
+        count_finish();
+        bs->resumes++;
+      }
+    }
   }
-  ck(batch_unpack(dmem, B, MB, NB, X, ldp, sP, Hp, ldn, sN, st));
-  c.stats.launches++;
   for (int b = 0; b < B; ++b)
     if (iterations) iterations[idx[b]] = its[b];
   bs->buckets++;
@@ -1069,6 +1324,9 @@ int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* 
           ck(cudaSetDevice(wc.device()));
           ck(cudaStreamWaitEvent(wc.stream(), ready, 0));
           wc.stats = Stats{};
+          wc.batch_graph = c.batch_graph;
+          wc.inject_chol_fail = c.inject_chol_fail;
+          wc.inject_batch_err = c.inject_batch_err;
           for (int b : assign[w])
             qdwh_bucket(wc, plan.members[b], plan.mb[b], plan.nb[b], m, n, dA, lda, dQ, ldq, dH, ldh, info,
                         iterations, &wbs[w]);
@@ -1093,6 +1351,12 @@ int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* 
       bs->max_iterations = std::max(bs->max_iterations, wbs[w].max_iterations);
       bs->flops += wbs[w].flops;
       bs->flops_useful += wbs[w].flops_useful;
+      bs->graph_replays += wbs[w].graph_replays;
+      bs->graph_captures += wbs[w].graph_captures;
+      bs->eager_scheduled += wbs[w].eager_scheduled;
+      bs->sync_loops += wbs[w].sync_loops;
+      bs->restarts += wbs[w].restarts;
+      bs->resumes += wbs[w].resumes;
       c.stats.launches += wl[w];
     }
   }

@@ -73,6 +73,13 @@ struct BatchStats {
   double flops_useful = 0.0;  // the same work counted on the unpadded sizes
   double ms = 0.0;
   double predicted_ms = 0.0;  // the bucket plan's predicted time (cost model)
+  // buckets by how their iterations ran (ZOLO_OPT_BATCH_GRAPH)
+  int graph_replays = 0;    // a cached graph launched
+  int graph_captures = 0;   // captured, instantiated and launched
+  int eager_scheduled = 0;  // the schedule's launches issued eagerly (first call of a shape)
+  int sync_loops = 0;       // the host-synchronized loop (option off, or profiling)
+  int restarts = 0;         // a Cholesky step failed: rerun through the synchronized loop
+  int resumes = 0;          // a member continued in the synchronized loop after the schedule
 };
 int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* const* dA, const int64_t* lda,
                double* const* dQ, const int64_t* ldq, double* const* dH, const int64_t* ldh, int* info,
