@@ -319,6 +319,16 @@ int zolo_batch_autotune(zolo_handle_t h, double* model);
 int zolo_batch_set_model(zolo_handle_t h, const double* model);
 int zolo_batch_plan(int count, const int* m, const int* n, const double* model, int max_batch, int mode,
                     int* bucket, int* mb, int* nb, double* predicted_ms);
+/* Step schedule of one bucket of zolo_qdwh_batch_dev (host only, no GPU): for `count`
+ * members with lower bounds l0[b] (PQDWHFACS's L after the bounds; a member with l0 outside
+ * (0, 1] takes no step) and IT limit maxit (12 in the solver), *steps receives the number of
+ * steps K; when K <= max_steps, qr[k] = 1 for a QR-form step, table[k*5*count + ...] the
+ * step's coefficients (count each: c or 1/sqrt(c), cx, cz, an error slot, the conditional
+ * flag), ucount[b] member b's unconditional steps, last[b] its last unconditional step and
+ * cond[b] its conditional step (-1 = none; see ZOLO_OPT_BATCH_GRAPH).  Output arrays may be
+ * NULL.  Returns 0, -2 bad argument, -3 bad maxit, -4 more than max_steps steps. */
+int zolo_batch_schedule(int count, const double* l0, int maxit, int max_steps, int* steps, int* qr, double* table,
+                        int* ucount, int* last, int* cond);
 /* The reference driver's sequence in one call (test_zolodrv1.f90:167-198: the bounds,
  * then PZOLOPD1 with SYM = 'N'), plus H when dH is not NULL: alpha = ||A||_F and
  * beta = 1/(sqrt(n) ||R^{-1}||_1) as zolo_bounds_dev mode 1, then Zolo-PD with rk

@@ -179,7 +179,7 @@ def hfunc(x: float) -> float:
 def qdwh_weights(lowk: float) -> tuple[float, float, float, float]:
     """a_k, b_k, c_k and the next lower bound (pqdwhfacs.f90:361-368)."""
     ak = hfunc(lowk)
-    bk = (ak - 1.0) ** 2 / 4.0
+    bk = (ak - 1.0) * (ak - 1.0) / 4.0  # Fortran (AK-1)**2 with an integer power is a product
     ck = ak + bk - 1.0
     l2 = lowk * lowk
     lnext = lowk * (ak + bk * l2) / (1.0 + ck * l2)

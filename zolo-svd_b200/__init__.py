@@ -123,6 +123,8 @@ _SIGS = [
                                   C.c_int, C.c_int, C.c_int]),
     ("zolo_batch_autotune", C.c_int, [C.c_void_p, c_double_p]),
     ("zolo_batch_stats", C.c_int, [C.c_void_p, c_double_p]),
+    ("zolo_batch_schedule", C.c_int, [C.c_int, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p, c_double_p, c_int_p,
+                                      c_int_p, c_int_p]),
     ("zolo_batch_set_model", C.c_int, [C.c_void_p, c_double_p]),
     ("zolo_batch_plan", C.c_int, [C.c_int, c_int_p, c_int_p, c_double_p, C.c_int, C.c_int, c_int_p, c_int_p,
                                   c_int_p, c_double_p]),
@@ -501,6 +503,25 @@ def qdwh_batch_dev(h: Handle, members, with_h: bool = True):
 
 BATCH_STATS_KEYS = ("buckets", "max_iterations", "flops", "flops_useful", "ms", "predicted_ms", "graph_replays",
                     "graph_captures", "eager_scheduled", "sync_loops", "restarts", "resumes")
+
+
+def batch_schedule(l0, maxit: int = 12) -> dict:
+    """Step schedule of one batched bucket for members with lower bounds l0
+    (zolo_batch_schedule; host only)."""
+    k = len(l0)
+    l = (C.c_double * max(k, 1))(*l0)
+    steps = C.c_int()
+    r = lib().zolo_batch_schedule(k, l, maxit, 0, C.byref(steps), None, None, None, None, None)
+    if r not in (0, -4):
+        raise ZoloError("zolo_batch_schedule", r)
+    K = steps.value
+    qr = (C.c_int * max(K, 1))()
+    tab = (C.c_double * max(5 * k * K, 1))()
+    uc, last, cond = (C.c_int * max(k, 1))(), (C.c_int * max(k, 1))(), (C.c_int * max(k, 1))()
+    _ck("zolo_batch_schedule", lib().zolo_batch_schedule(k, l, maxit, K, C.byref(steps), qr, tab, uc, last, cond))
+    import numpy as _np
+    return {"steps": K, "qr": list(qr)[:K], "table": _np.array(tab[:5 * k * K]).reshape(K, 5, k),
+            "count": list(uc)[:k], "last": list(last)[:k], "cond": list(cond)[:k]}
 
 
 def batch_stats(h: Handle) -> dict:

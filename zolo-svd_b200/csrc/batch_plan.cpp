@@ -2,9 +2,12 @@
 #include "batch_plan.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <limits>
 #include <numeric>
+
+#include "coeff.h"
 
 namespace zolo {
 
@@ -133,6 +136,62 @@ BucketPlan ladder_buckets(const BatchCostModel& mdl, int count, const int* m, co
   }
   p.total_ms = plan_predicted_ms(mdl, p);
   return p;
+}
+
+QdwhSchedule qdwh_schedule(int B, const double* l0, const char* done, double tol1, int maxit) {
+  QdwhSchedule S;
+  S.count.assign(B, 0);
+  S.last.assign(B, -1);
+  S.cond.assign(B, -1);
+  S.l_uncond.assign(l0, l0 + B);
+  S.l_cond.assign(l0, l0 + B);
+  std::vector<char> act(B), pend(B, 0);
+  std::vector<double> l(l0, l0 + B), ak(B), bk(B), ck(B), ln(B);
+  for (int b = 0; b < B; ++b) act[b] = !done[b];
+  while (true) {
+    bool any = false, qr = false;
+    for (int b = 0; b < B; ++b) {
+      if (!act[b]) continue;
+      any = true;
+      qdwh_weights(l[b], &ak[b], &bk[b], &ck[b], &ln[b]);
+      qr = qr || ck[b] > 100.0;
+    }
+    if (!any) break;
+    const int k = S.steps++;
+    S.qr.push_back(qr);
+    S.table.resize(static_cast<size_t>(k + 1) * 5 * B, 0.0);
+    double* row = S.table.data() + static_cast<size_t>(k) * 5 * B;
+    for (int b = 0; b < B; ++b) {
+      if (!act[b]) {
+        row[b] = qr ? 1.0 : 0.0;
+        row[B + b] = 1.0;
+        row[2 * B + b] = 0.0;
+        continue;
+      }
+      const double sck = std::sqrt(ck[b]);
+      row[b] = qr ? 1.0 / sck : ck[b];
+      row[B + b] = bk[b] / ck[b];
+      row[2 * B + b] = qr ? (ak[b] - bk[b] / ck[b]) / sck : ak[b] - bk[b] / ck[b];
+      l[b] = ln[b];
+      if (pend[b]) {  // the conditional step: the member's last scheduled one
+        row[4 * B + b] = 1.0;
+        S.cond[b] = k;
+        S.l_cond[b] = l[b];
+        act[b] = 0;
+        continue;
+      }
+      ++S.count[b];
+      S.l_uncond[b] = l[b];
+      S.l_cond[b] = l[b];
+      S.last[b] = k;
+      if (S.count[b] > maxit) {
+        act[b] = 0;
+      } else if (!(std::fabs(1.0 - l[b]) > tol1)) {
+        pend[b] = 1;
+      }
+    }
+  }
+  return S;
 }
 
 }  // namespace zolo

@@ -43,4 +43,26 @@ BucketPlan ladder_buckets(const BatchCostModel& mdl, int count, const int* m, co
 // least loaded worker): the sum of the work plus the largest per-worker latency chain.
 double plan_predicted_ms(const BatchCostModel& mdl, const BucketPlan& p);
 
+// Step schedule of one bucket of B members (PQDWHFACS, pqdwhfacs.f90:359-372 per member),
+// computed before any step runs: L_k of a member follows from L_0 alone, so every step's
+// form and weights are known in advance.  A member steps unconditionally while
+// |1 - L| > tol1 and IT <= maxit; once L has converged it takes one more step only while its
+// error (measured on the device) is above TOL1^(1/3): that step is scheduled as conditional.
+// Step k is the QR form when some member scheduled at k has c_k > 100.
+struct QdwhSchedule {
+  int steps = 0;
+  std::vector<char> qr;           // per step: 1 = QR form, 0 = Cholesky form
+  // per step 5 B doubles: the form's coefficient (c, or 1/sqrt(c) for the QR stack),
+  // cx = b/c, cz = a - b/c (divided by sqrt(c) in the QR form), an error slot (0) and the
+  // conditional flag; members not scheduled at a step get the neutral values (0 or 1, 1, 0)
+  std::vector<double> table;
+  std::vector<int> count;         // per member: unconditional steps
+  std::vector<int> last;          // per member: its last unconditional step (-1 = none)
+  std::vector<int> cond;          // per member: its conditional step (-1 = none)
+  std::vector<double> l_uncond;   // per member: L after its last unconditional step
+  std::vector<double> l_cond;     // per member: L after its conditional step
+};
+// done[b] != 0: member b takes no step (its bounds failed).
+QdwhSchedule qdwh_schedule(int B, const double* l0, const char* done, double tol1, int maxit);
+
 }  // namespace zolo

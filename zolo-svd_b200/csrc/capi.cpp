@@ -564,6 +564,29 @@ int zolo_batch_plan(int count, const int* m, const int* n, const double* model, 
   return static_cast<int>(p.members.size());
 }
 
+int zolo_batch_schedule(int count, const double* l0, int maxit, int max_steps, int* steps, int* qr, double* table,
+                        int* ucount, int* last, int* cond) {
+  if (count < 0 || max_steps < 0 || !steps || (count > 0 && !l0)) return -2;
+  if (maxit < 0 || maxit > 100) return -3;
+  std::vector<char> done(count);
+  for (int b = 0; b < count; ++b) done[b] = !(l0[b] > 0.0 && l0[b] <= 1.0);
+  const zolo::QdwhSchedule S = zolo::qdwh_schedule(count, l0, done.data(), 10.0 * zolo::eps_precision() / 2.0, maxit);
+  *steps = S.steps;
+  if (S.steps > max_steps) return -4;
+  for (int k = 0; k < S.steps; ++k) {
+    if (qr) qr[k] = S.qr[k];
+    if (table)
+      for (size_t i = 0; i < static_cast<size_t>(5) * count; ++i)
+        table[static_cast<size_t>(k) * 5 * count + i] = S.table[static_cast<size_t>(k) * 5 * count + i];
+  }
+  for (int b = 0; b < count; ++b) {
+    if (ucount) ucount[b] = S.count[b];
+    if (last) last[b] = S.last[b];
+    if (cond) cond[b] = S.cond[b];
+  }
+  return 0;
+}
+
 int zolo_polar_dev(zolo_handle_t h, int rk, int m, int n, const double* dA, int64_t lda, double* dQ, int64_t ldq,
                    double* dH, int64_t ldh) {
   if (m < n) return -3;

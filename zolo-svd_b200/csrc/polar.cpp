@@ -1046,62 +1046,18 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
     count_finish();
     bs->sync_loops++;
   } else {
-    // The schedule: L_k of every member follows from its L_0 alone (the weights of
-    // pqdwhfacs.f90:362-372), so the host computes every step's form and coefficients before
-    // the first one runs.  A member continues unconditionally while |1 - L| > TOL1 (and
-    // IT <= 12); once L has converged, the loop continues only while ERR > TOL1^(1/3), a value
-    // the device measures: that next step is scheduled as conditional, and a gate kernel
-    // makes it neutral for the member when the previous step's error is already below.
-    std::vector<char> act(B), sqr, pend(B, 0), hascond(B, 0);
-    for (int b = 0; b < B; ++b) act[b] = !done[b];
-    std::vector<double> l = lowk, lu = lowk, tab;
-    std::vector<int> cnt(B, 0), last(B, -1), kc(B, -1);
-    while (true) {
-      bool any = false, qr = false;
-      for (int b = 0; b < B; ++b) {
-        if (!act[b]) continue;
-        any = true;
-        qdwh_weights(l[b], &ak[b], &bk[b], &ckv[b], &ln[b]);
-        qr = qr || ckv[b] > 100.0;
-      }
-      if (!any) break;
-      const int k = static_cast<int>(sqr.size());
-      sqr.push_back(qr);
-      tab.resize(static_cast<size_t>(k + 1) * 5 * B, 0.0);
-      double* row = tab.data() + static_cast<size_t>(k) * 5 * B;
-      for (int b = 0; b < B; ++b) {
-        if (!act[b]) {
-          row[b] = qr ? 1.0 : 0.0;
-          row[B + b] = 1.0;
-          row[2 * B + b] = 0.0;
-          continue;
-        }
-        const double sck = std::sqrt(ckv[b]);
-        row[b] = qr ? 1.0 / sck : ckv[b];
-        row[B + b] = bk[b] / ckv[b];
-        row[2 * B + b] = qr ? (ak[b] - bk[b] / ckv[b]) / sck : ak[b] - bk[b] / ckv[b];
-        l[b] = ln[b];
-        if (pend[b]) {  // the conditional step: the member's last scheduled one
-          row[4 * B + b] = 1.0;
-          kc[b] = k;
-          hascond[b] = 1;
-          act[b] = 0;
-          continue;
-        }
-        ++cnt[b];
-        lu[b] = l[b];
-        last[b] = k;
-        if (cnt[b] > maxit) {
-          act[b] = 0;
-        } else if (!(std::fabs(1.0 - l[b]) > tol1)) {
-          pend[b] = 1;
-        }
-      }
-    }
-    const int K = static_cast<int>(sqr.size());
+    // The schedule (qdwh_schedule): every step's form and weights from the members' L_0; a
+    // step after a member's L has converged is conditional, and a gate kernel makes it neutral
+    // for the member on the device when the error just measured is already below TOL1^(1/3).
+    const QdwhSchedule S = qdwh_schedule(B, lowk.data(), done.data(), tol1, maxit);
+    const int K = S.steps;
+    const std::vector<char>& sqr = S.qr;
+    const std::vector<int>&cnt = S.count, &last = S.last, &kc = S.cond;
+    std::vector<char> hascond(B);
+    for (int b = 0; b < B; ++b) hascond[b] = kc[b] >= 0;
     double* sched = c.buf("bat_sched", static_cast<size_t>(std::max(K, 1)) * 5 * B);
     int* sinfo = c.ibuf("bat_sinfo", static_cast<size_t>(std::max(K, 1)) * B);
-    if (K > 0) h2d(c, sched, tab.data(), K * 5 * B);
+    if (K > 0) h2d(c, sched, S.table.data(), K * 5 * B);
     std::vector<char> gated(K, 0);
     for (int b = 0; b < B; ++b)
       if (kc[b] >= 0) gated[kc[b]] = 1;
@@ -1248,7 +1204,7 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
         if (last[b] < 0) continue;
         const int kf = took[b] ? kc[b] : last[b];
         its[b] = cnt[b] + (took[b] ? 1 : 0);
-        lowk[b] = took[b] ? l[b] : lu[b];
+        lowk[b] = took[b] ? S.l_cond[b] : S.l_uncond[b];
         err[b] = std::sqrt(e2_at(kf, b));
         // pqdwhfacs.f90:359 after the member's last step
         const bool high = err[b] > tol2 || (c.inject_batch_err && b == 0);
