@@ -419,7 +419,7 @@ def bench_batch_c4(torch, zb, h, reps: int = 3) -> dict:
            "tflops_executed": st["flops_executed"] / (ms * 1e-3) / 1e12,
            "worst_backward_error_over_10neps": worst_b, "worst_orthogonality_over_10neps": worst_o,
            "worst_sv_err_rel_smax": worst_s,
-           "launch": "one CUDA graph per bucket (iterations, H, unpacking) replayed on four worker streams; "
+           "launch": "one CUDA graph per bucket (iterations, H, unpacking) replayed on eight worker streams; "
                      "bounds eager", "buckets": gst["buckets"], "graph_replays": gst["graph_replays"],
            "ms_first_call_eager": ms_first, "ms_capture_call": ms_capture, "ms_synchronized_loop": ms_sync}
     del da, dq, dh

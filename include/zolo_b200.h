@@ -356,7 +356,10 @@ int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq
 /* Symmetric eigendecomposition H = Z diag(w) Z^T (n x n), w ascending: the replacement
  * of ELPA_PDSYEVD2 (elpa_pdsyevd2.F90:199-200) -- spectral divide-and-conquer on the
  * polar decomposition (QDWH of H - sigma I, subspace split as pqdwhsubit.f90:227-312,
- * recursively) with batched Jacobi leaves.  Returns 0, or > 0 if no split point worked. */
+ * recursively) with batched Jacobi leaves.  Returns 0, or > 0 if no split point worked.
+ * zolo_get_stats afterwards: iterations = splits, qr_iterations = QDWH iterations,
+ * chol_iterations = leaves, last_err = largest split residual / ||H||_F, ms_step[l] = device
+ * ms of top-down level l, ms_finish = the leaves, ms_h = the back-transformation. */
 int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz);
 /* Zolo-SVD (test_zolodrv1.f90 + ZoloCHK1.f90:80-91): A = U diag(s) V^T for m >= n via
  * QDWH-PD (algo 0) or Zolo-PD with rk terms (algo 1), H = sym(Q^T A), H = V diag(s) V^T,

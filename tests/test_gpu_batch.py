@@ -157,6 +157,36 @@ def test_batch_graph_recovery_paths(inject):
     h.close()
 
 
+def test_batch_autotune_model():
+    """zolo_batch_autotune measures a cost model within the FP64 tensor path's range (latency
+    terms >= 0, 0.5 < rate < 60 TF/s) whose plan solves a batch correctly and not much slower
+    than the default model's plan."""
+    import ctypes as C
+    import time
+    import torch
+    h = zb.Handle(0)
+    mats = _members(5, 48, 24, 400)
+    tuned = (C.c_double * 5)()
+    assert zb.lib().zolo_batch_autotune(h.ptr, tuned) == 0
+    lat0, lat1, rate, nhalf, streams = list(tuned)
+    assert lat0 >= 0 and lat1 >= 0 and 0.5 < rate < 60 and 0 <= nhalf < 8192 and streams >= 1
+    times = {}
+    for name, md in (("default", (4.0, 0.35, 25.0, 384.0, 8.0)), ("tuned", tuple(tuned))):
+        assert zb.lib().zolo_batch_set_model(h.ptr, (C.c_double * 5)(*md)) == 0
+        for _ in range(2):
+            _run_batch(h, mats)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info, its, qs, hs = _run_batch(h, mats)
+        times[name] = time.perf_counter() - t0
+        assert info == [0] * len(mats)
+        for (a, uv, s, kappa), q, hh in zip(mats, qs, hs):
+            n = a.shape[1]
+            assert zo.backward_error(a, q, hh) <= tol_n(n) and zo.orthogonality(q) <= tol_n(n)
+    assert times["tuned"] <= 1.6 * times["default"], times
+    h.close()
+
+
 def config4_members(seed=1004, count=512):
     """Configuration 4: n = round(exp U[ln 64, ln 1024]), m = round(n (1 + U[0, 1])),
     kappa = 10^U[2, 14], s geometric from 1 to 1/kappa; member i generated from PCG64 seed

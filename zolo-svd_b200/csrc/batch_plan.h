@@ -17,7 +17,7 @@ struct BatchCostModel {
   double lat1 = 0.35;
   double rate_tflops = 25.0;
   double nhalf = 384.0;
-  int streams = 4;  // worker streams the buckets are spread over
+  int streams = 8;  // worker streams the buckets are spread over
 };
 
 // Executed FP64 flops of one padded member's PQDWHFACS solve (bounds, two QR-form and four

@@ -631,6 +631,11 @@ int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double*
     c.stats.chol_iterations = es.leaves;
     c.stats.last_err = es.max_split_residual;
     c.stats.flops = es.flops;
+    // device ms: ms_step[l] = top-down level l, ms_finish = leaves, ms_h = back-transformation
+    for (int l = 0; l < std::min(es.levels, 16); ++l) c.stats.ms_step[l] = es.ms_level[l];
+    c.stats.ms_finish = es.ms_leaves;
+    c.stats.ms_h = es.ms_back;
+    c.stats.ms_total = es.ms_total;
     return info;
   });
 }

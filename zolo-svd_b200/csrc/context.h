@@ -163,6 +163,30 @@ class Context {
   void* grow(const std::string& name, size_t bytes);
 };
 
+// Device time between construction and stop() on one stream (CUDA events; stop() waits).
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    ck(cudaEventCreate(&a));
+    ck(cudaEventCreate(&b));
+    ck(cudaEventRecord(a, s));
+  }
+  double stop() {
+    ck(cudaEventRecord(b, s));
+    ck(cudaEventSynchronize(b));
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+  EventTimer(const EventTimer&) = delete;
+  EventTimer& operator=(const EventTimer&) = delete;
+  ~EventTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 // Routes the large products of gemm() to the INT8-emulated GEMM while in scope (when the
 // handle's mixed form is on), and restores the previous routing on exit.
 struct OzScope {

@@ -220,6 +220,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   EigStats local;
   EigStats& S = es ? *es : local;
   S = EigStats{};
+  EventTimer total(c.stream());
   DevMem mem;
   std::vector<Node> nodes;
   {
@@ -240,6 +241,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     const size_t hi = nodes.size();
     levels.emplace_back(lo, hi);
     const int cnt = static_cast<int>(hi - lo);
+    EventTimer tl(c.stream());
     std::vector<Node> kids(2 * cnt);
     std::vector<EigStats> st(cnt);
     std::vector<char> ok(cnt, 1);
@@ -255,6 +257,9 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
       S.flops += st[i].flops;
       S.max_split_residual = std::max(S.max_split_residual, st[i].max_split_residual);
     }
+    const double ms_lv = tl.stop();
+    if (S.levels < 16) S.ms_level[S.levels] = ms_lv;
+    S.levels++;
     for (int i = 0; i < cnt; ++i)
       if (!ok[i]) return 2;  // no usable split point (all candidates failed)
     for (int i = 0; i < cnt; ++i) {
@@ -276,6 +281,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   for (auto& nd : nodes)
     if (nd.leaf) leaves.push_back(JacobiLeaf{nd.H, nd.ld, nd.n, nd.w, nd.Z, even(nd.n)});
   S.leaves = static_cast<int>(leaves.size());
+  EventTimer tleaf(c.stream());
   {
     void* dl = nullptr;
     ck(cudaMalloc(&dl, sizeof(JacobiLeaf) * leaves.size()));
@@ -288,6 +294,8 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     ck(cudaStreamSynchronize(c.stream()));
     for (int s : sw) S.max_jacobi_sweeps = std::max(S.max_jacobi_sweeps, s);
   }
+  S.ms_leaves = tleaf.stop();
+  EventTimer tback(c.stream());
 
   // ---- bottom-up back-transformation, one level at a time (concurrent within a level) ----
   for (auto lv = levels.rbegin(); lv != levels.rend(); ++lv) {
@@ -313,6 +321,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     }
   }
 
+  S.ms_back = tback.stop();
   // ---- ascending order (dsyevd / ELPA convention) ----
   const Node& root = nodes[0];
   std::vector<double> w(n);
@@ -327,7 +336,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   ck(cudaMemcpyAsync(dperm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream()));
   ck(cudaMemcpyAsync(dW, ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c.stream()));
   ck(gather_columns(n, n, root.Z, even(n), dperm, dZ, ldz, c.stream()));
-  ck(cudaStreamSynchronize(c.stream()));
+  S.ms_total = total.stop();
   return 0;
 }
 

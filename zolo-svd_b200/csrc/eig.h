@@ -18,6 +18,11 @@ struct EigStats {
   int max_jacobi_sweeps = 0;
   double max_split_residual = 0.0;  // max ||V2^T H V1||_F / ||H||_F over the splits
   double flops = 0.0;
+  // device ms (CUDA events on the calling stream): each top-down level's splits, the
+  // Jacobi leaves, the bottom-up back-transformation, the whole call
+  int levels = 0;
+  double ms_level[16] = {0};
+  double ms_leaves = 0.0, ms_back = 0.0, ms_total = 0.0;
 };
 
 // H = Z diag(w) Z^T for symmetric H (n x n); w ascending.  Returns 0 or > 0 on failure.
