@@ -130,11 +130,34 @@ void run_concurrent(Context& c, int count, F&& task) {
     if (err[w] != cudaSuccess) throw CudaFailure{err[w]};
 }
 
+// Candidate shifts of a node from its diagonal: the median and the mean, then the median
+// nudged by 1e-3 of the diagonal's span either way.
+void split_candidates(const std::vector<double>& dg, double cand[4]) {
+  const int m = static_cast<int>(dg.size());
+  std::vector<double> srt = dg;
+  std::sort(srt.begin(), srt.end());
+  const double med = srt[m / 2], mean = std::accumulate(dg.begin(), dg.end(), 0.0) / m;
+  const double span = std::max(srt.back() - srt.front(), 1e-300);
+  cand[0] = 0.5 * (srt[(m - 1) / 2] + srt[m / 2]);
+  cand[1] = mean;
+  cand[2] = med + 1e-3 * span;
+  cand[3] = med - 1e-3 * span;
+}
+
+// The polar factor of H - sigma I for the first candidate shift, computed before the node is
+// split (the level's nodes in one batched solve): Up (ld even(m)), or info != 0 if it failed.
+struct Presolved {
+  const double* Up = nullptr;
+  int info = 1;
+};
+
 // One node of the divide-and-conquer: a leaf (m <= kJacobiLeaf) or a split into the blocks of
 // V^T H V above and below a shift (QDWH polar factor of H - sigma I, subspace basis of its
 // projector).  Fills nd (k, V, Z, w) and the children L, R; returns false if no candidate
-// shift splits the spectrum.
-bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnorm, uint64_t seed, EigStats& S) {
+// shift splits the spectrum.  dg: the node's diagonal (empty for a leaf); pre: the first
+// candidate's polar factor when already computed.
+bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnorm, uint64_t seed, EigStats& S,
+                const std::vector<double>& dg, const Presolved& pre) {
   const double eps = 2.220446049250313e-16;
   const int m = nd.n;
   const int64_t ldm = even(m);
@@ -144,37 +167,34 @@ bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnor
     nd.leaf = true;
     return true;
   }
-  // split points: median and mean of the diagonal, then nudged versions
-  std::vector<double> dg(m);
-  double* dd = c.buf("eig_diag", m);
-  ck(get_diag(m, nd.H, nd.ld, dd, c.stream()));
-  ck(cudaMemcpyAsync(dg.data(), dd, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream()));
-  ck(cudaStreamSynchronize(c.stream()));
-  std::vector<double> srt = dg;
-  std::sort(srt.begin(), srt.end());
-  const double med = srt[m / 2], mean = std::accumulate(dg.begin(), dg.end(), 0.0) / m;
-  const double span = std::max(srt.back() - srt.front(), 1e-300);
-  const double cand[4] = {0.5 * (srt[(m - 1) / 2] + srt[m / 2]), mean, med + 1e-3 * span, med - 1e-3 * span};
+  double cand[4];
+  split_candidates(dg, cand);
   nd.V = mem.alloc(static_cast<size_t>(ldm) * m);
   double* Up = c.buf("eig_up", static_cast<size_t>(ldm) * m);
   double* P = c.buf("eig_p", static_cast<size_t>(ldm) * m);
   double* X = c.buf("eig_x", static_cast<size_t>(ldm) * m);
   double* E = c.buf("eig_e", static_cast<size_t>(ldm) * m);
   for (int a = 0; a < 4; ++a) {
-    QdwhOpts o;
-    o.sym = 'N';
-    o.sigma = cand[a];
-    o.bounds = BOUNDS_PQDWHFACS;
-    o.maxit = 12;
-    const Stats saved = c.stats;
-    const int info = qdwh(c, m, m, nd.H, nd.ld, Up, ldm, nullptr, 0, o);
-    S.qdwh_calls++;
-    S.qdwh_iterations += c.stats.iterations;
-    S.flops += c.stats.flops;
-    c.stats = saved;
-    if (info != 0) continue;
+    const double* Ua = Up;
+    if (a == 0 && pre.Up) {
+      if (pre.info != 0) continue;
+      Ua = pre.Up;
+    } else {
+      QdwhOpts o;
+      o.sym = 'N';
+      o.sigma = cand[a];
+      o.bounds = BOUNDS_PQDWHFACS;
+      o.maxit = 12;
+      const Stats saved = c.stats;
+      const int info = qdwh(c, m, m, nd.H, nd.ld, Up, ldm, nullptr, 0, o);
+      S.qdwh_calls++;
+      S.qdwh_iterations += c.stats.iterations;
+      S.flops += c.stats.flops;
+      c.stats = saved;
+      if (info != 0) continue;
+    }
     // projector onto the eigenvalues above the split: P = (Up + I)/2, k = trace(P)
-    ck(scale_copy(m, m, 0.5, Up, ldm, 0, P, ldm, 0, 1, 0.5, c.stream()));
+    ck(scale_copy(m, m, 0.5, Ua, ldm, 0, P, ldm, 0, 1, 0.5, c.stream()));
     ck(trace(m, P, ldm, c.dscal() + 10, c.stream()));
     const int k = static_cast<int>(std::lround(d2h(c, c.dscal() + 10)));
     if (k <= 0 || k >= m) continue;
@@ -245,10 +265,81 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     std::vector<Node> kids(2 * cnt);
     std::vector<EigStats> st(cnt);
     std::vector<char> ok(cnt, 1);
+    // the diagonals of the level's inner nodes (one read-back), their candidate shifts
+    std::vector<std::vector<double>> dg(cnt);
+    std::vector<int> inner;
+    {
+      size_t tot = 0;
+      for (int i = 0; i < cnt; ++i)
+        if (nodes[lo + i].n > kJacobiLeaf) {
+          inner.push_back(i);
+          tot += nodes[lo + i].n;
+        }
+      double* dd = c.buf("eig_diag", std::max<size_t>(tot, 1));
+      std::vector<double> hd(tot);
+      size_t off = 0;
+      for (int i : inner) {
+        ck(get_diag(nodes[lo + i].n, nodes[lo + i].H, nodes[lo + i].ld, dd + off, c.stream()));
+        off += nodes[lo + i].n;
+      }
+      if (tot) {
+        ck(cudaMemcpyAsync(hd.data(), dd, sizeof(double) * tot, cudaMemcpyDeviceToHost, c.stream()));
+        ck(cudaStreamSynchronize(c.stream()));
+      }
+      off = 0;
+      for (int i : inner) {
+        dg[i].assign(hd.begin() + off, hd.begin() + off + nodes[lo + i].n);
+        off += nodes[lo + i].n;
+      }
+    }
+    // with two or more inner nodes, the QDWH of every node's H - sigma_0 I as one batched solve
+    // (zolo_qdwh_batch_dev's buckets and graphs; PQDWHFACS bounds per member)
+    std::vector<Presolved> pre(cnt);
+    double* arena = nullptr;
+    if (inner.size() >= 2) {
+      size_t tot = 0;
+      for (int i : inner) tot += 2 * static_cast<size_t>(even(nodes[lo + i].n)) * nodes[lo + i].n;
+      arena = mem.alloc(tot);
+      const int nb = static_cast<int>(inner.size());
+      std::vector<int> mm(nb), inf(nb, 0), its(nb, 0);
+      std::vector<const double*> pa(nb);
+      std::vector<double*> pq(nb);
+      std::vector<int64_t> ld(nb);
+      size_t off = 0;
+      for (int j = 0; j < nb; ++j) {
+        const Node& nd = nodes[lo + inner[j]];
+        const int64_t ldm = even(nd.n);
+        double cand[4];
+        split_candidates(dg[inner[j]], cand);
+        double* Hs = arena + off;
+        double* Up = Hs + ldm * nd.n;
+        off += 2 * static_cast<size_t>(ldm) * nd.n;
+        ck(scale_copy(nd.n, nd.n, 1.0, nd.H, nd.ld, 0, Hs, ldm, 0, 1, 0.0, c.stream()));
+        ck(add_diag(nd.n, Hs, ldm, -cand[0], c.stream()));
+        mm[j] = nd.n;
+        pa[j] = Hs;
+        pq[j] = Up;
+        ld[j] = ldm;
+      }
+      BatchStats bs;
+      const Stats saved = c.stats;
+      const int rb = qdwh_batch(c, nb, mm.data(), mm.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
+                                nullptr, inf.data(), its.data(), &bs);
+      c.stats = saved;
+      if (rb != 0) std::fill(inf.begin(), inf.end(), 1);  // each node then solves on its own
+      S.qdwh_calls += nb;
+      for (int j = 0; j < nb; ++j) {
+        S.qdwh_iterations += its[j];
+        pre[inner[j]] = Presolved{pq[j], inf[j]};
+      }
+      S.flops += bs.flops_useful;
+      S.batched_nodes += nb;
+    }
     run_concurrent(c, cnt, [&](Context& wc, int i) {
       ok[i] = split_node(wc, nodes[lo + i], kids[2 * i], kids[2 * i + 1], mem, hnorm,
-                         0x5EEDull + (lo + i) * 7919ull, st[i]) ? 1 : 0;
+                         0x5EEDull + (lo + i) * 7919ull, st[i], dg[i], pre[i]) ? 1 : 0;
     });
+    if (arena) mem.release(arena);
     for (int i = 0; i < cnt; ++i) {
       S.qdwh_calls += st[i].qdwh_calls;
       S.qdwh_iterations += st[i].qdwh_iterations;

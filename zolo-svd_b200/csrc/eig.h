@@ -18,6 +18,7 @@ struct EigStats {
   int max_jacobi_sweeps = 0;
   double max_split_residual = 0.0;  // max ||V2^T H V1||_F / ||H||_F over the splits
   double flops = 0.0;
+  int batched_nodes = 0;  // nodes whose first-candidate QDWH ran in a level's batched solve
   // device ms (CUDA events on the calling stream): each top-down level's splits, the
   // Jacobi leaves, the bottom-up back-transformation, the whole call
   int levels = 0;
