@@ -140,7 +140,7 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * counts.  No reference counterpart. */
 #define ZOLO_OPT_TERM_PLAN 5
 /* ZOLO_OPT_MIXED: 0 (default) = every matrix product on the FP64 tensor path (DMMA);
- * 1 = the mixed form: the large products (K >= 256 and at least one wave of output tiles)
+ * 1 = the mixed form: the large products (K >= 256 and at least two waves of output tiles)
  * of the Cholesky-form iterations, of the Newton-Schulz finish and of forming Q and H run
  * on the INT8 tensor cores with the FP64 product emulated from ZOLO_OPT_MIXED_SLICES digit
  * planes per operand (zolo_ozgemm_dev); the bounds and the QR-form iterations stay on the
@@ -192,6 +192,12 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * scheduled run sees the first member of each bucket with its last error above TOL1^(1/3), so
  * that member continues in the synchronized loop.  Host-side only. */
 #define ZOLO_OPT_INJECT_BATCH_ERR 12
+/* ZOLO_OPT_EIG_ZOLO_MIN: the eigensolver (zolo_syev_dev, zolo_svd_dev) splits a node of size
+ * n >= this value (default 4096) at its first candidate shift with the polar factor of
+ * H - sigma I from Zolo-PD (r = 8 with every cost option: about 0.7x QDWH's time at n = 8192);
+ * smaller nodes use QDWH, those of one recursion level as one batched solve; 0 = QDWH for
+ * every node (pqdwhsubit.f90's polar factor).  The later candidate shifts always use QDWH. */
+#define ZOLO_OPT_EIG_ZOLO_MIN 13
 /* The default handle (used by the reference-named host-array entry points) reads its options
  * from the environment when it is created, so an unchanged Fortran driver selects them:
  * ZOLO_FAST=1 sets ZOLO_OPT_SHARED_QR, _NS_FINISH, _CHOL_INVERSE, _BETA_FROB, _TERM_PLAN and
@@ -359,7 +365,9 @@ int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq
  * recursively) with batched Jacobi leaves.  Returns 0, or > 0 if no split point worked.
  * zolo_get_stats afterwards: iterations = splits, qr_iterations = QDWH iterations,
  * chol_iterations = leaves, last_err = largest split residual / ||H||_F, ms_step[l] = device
- * ms of top-down level l, ms_finish = the leaves, ms_h = the back-transformation. */
+ * ms of top-down level l, ms_finish = the leaves, ms_h = the back-transformation,
+ * ns_steps = subspace passes, terms[0..2] = QDWH solves, Zolo-PD solves, nodes solved in
+ * a level's batched QDWH. */
 int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz);
 /* Zolo-SVD (test_zolodrv1.f90 + ZoloCHK1.f90:80-91): A = U diag(s) V^T for m >= n via
  * QDWH-PD (algo 0) or Zolo-PD with rk terms (algo 1), H = sym(Q^T A), H = V diag(s) V^T,

@@ -61,6 +61,33 @@ def test_syev_vs_lapack(h, n):
     assert np.linalg.norm(z.T @ z - np.eye(n)) / math.sqrt(n) <= tol_n(n)
 
 
+@pytest.mark.parametrize("zolo_min", [0, 96])
+@pytest.mark.parametrize("n", [150, 301])
+def test_syev_split_polar_forms(n, zolo_min):
+    """ZOLO_OPT_EIG_ZOLO_MIN: with 0 every node splits on QDWH polar factors (a level's nodes
+    in one batched solve); with 96 the nodes of at least 96 rows split on Zolo-PD's (fast
+    form) and the smaller ones on batched QDWH.  Both agree with LAPACK dsyevd; the split
+    statistics show which solvers ran."""
+    hd = zb.Handle(0)
+    hd.set_option(zb.OPT_EIG_ZOLO_MIN, zolo_min)
+    rng = np.random.default_rng(1000 + n)
+    # a spectrum symmetric about 0, so that the median shifts split the nodes in halves
+    lam = np.sort(np.concatenate([np.linspace(-1.0, 1.0, n - 8), rng.uniform(-1e-3, 1e-3, 8)]))
+    a = _sym_with_spectrum(n, lam, 40 + n)
+    w, z = _syev(hd, a)
+    st = hd.stats()
+    qdwh_calls, zolo_calls, batched = st["terms"][:3]
+    if zolo_min == 0:
+        assert zolo_calls == 0 and qdwh_calls >= st["iterations"]
+    else:
+        assert zolo_calls >= 1  # the root (n >= 96) at least
+    assert batched >= 2
+    assert np.max(np.abs(w - np.sort(lam))) <= 1e-12
+    assert np.linalg.norm(a @ z - z * w[None, :]) / np.linalg.norm(a) <= tol_n(n)
+    assert np.linalg.norm(z.T @ z - np.eye(n)) / math.sqrt(n) <= tol_n(n)
+    hd.close()
+
+
 def test_syev_clustered_spd_spectrum(h):
     """SPD H with 20% of the eigenvalues exactly 1 and tight clusters (relative gap 1e-9),
     the eigen-stage stress case of the full SVD workload, scaled down."""

@@ -165,6 +165,7 @@ OPT_INJECT_CHOL_FAIL = 9
 OPT_NORM2_BOUND = 10
 OPT_BATCH_GRAPH = 11
 OPT_INJECT_BATCH_ERR = 12
+OPT_EIG_ZOLO_MIN = 13
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
                    "ozgemm", "dgemm_k256"]
 

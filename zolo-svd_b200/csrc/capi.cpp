@@ -142,6 +142,10 @@ int set_option(Context& c, int option, int value) {
     case ZOLO_OPT_INJECT_BATCH_ERR:
       c.inject_batch_err = value != 0;
       return 0;
+    case ZOLO_OPT_EIG_ZOLO_MIN:
+      if (value < 0) return -3;
+      c.eig_zolo_min = value;
+      return 0;
     default:
       return -1;
   }
@@ -173,7 +177,8 @@ void apply_env_options(Context& c) {
       {"ZOLO_OPT_CHOL_INVERSE", ZOLO_OPT_CHOL_INVERSE}, {"ZOLO_OPT_BETA_FROB", ZOLO_OPT_BETA_FROB},
       {"ZOLO_OPT_TERM_PLAN", ZOLO_OPT_TERM_PLAN},   {"ZOLO_OPT_MIXED", ZOLO_OPT_MIXED},
       {"ZOLO_OPT_MIXED_SLICES", ZOLO_OPT_MIXED_SLICES}, {"ZOLO_OPT_OWN_BOUNDS", ZOLO_OPT_OWN_BOUNDS},
-      {"ZOLO_OPT_NORM2_BOUND", ZOLO_OPT_NORM2_BOUND},   {"ZOLO_OPT_BATCH_GRAPH", ZOLO_OPT_BATCH_GRAPH}};
+      {"ZOLO_OPT_NORM2_BOUND", ZOLO_OPT_NORM2_BOUND},   {"ZOLO_OPT_BATCH_GRAPH", ZOLO_OPT_BATCH_GRAPH},
+      {"ZOLO_OPT_EIG_ZOLO_MIN", ZOLO_OPT_EIG_ZOLO_MIN}};
   for (const auto& nm : names)
     if (get(nm.first, &v)) set_option(c, nm.second, v);
 }
@@ -342,6 +347,7 @@ int zolo_get_option(zolo_handle_t h, int option, int* value) {
       case ZOLO_OPT_NORM2_BOUND: *value = c.zolo_norm2; return 0;
       case ZOLO_OPT_BATCH_GRAPH: *value = c.batch_graph; return 0;
       case ZOLO_OPT_INJECT_BATCH_ERR: *value = c.inject_batch_err; return 0;
+      case ZOLO_OPT_EIG_ZOLO_MIN: *value = c.eig_zolo_min; return 0;
       default: return -1;
     }
   });
@@ -636,6 +642,10 @@ int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double*
     c.stats.ms_finish = es.ms_leaves;
     c.stats.ms_h = es.ms_back;
     c.stats.ms_total = es.ms_total;
+    c.stats.ns_steps = es.subspace_passes;
+    c.stats.terms[0] = es.qdwh_calls;
+    c.stats.terms[1] = es.zolo_calls;
+    c.stats.terms[2] = es.batched_nodes;
     return info;
   });
 }

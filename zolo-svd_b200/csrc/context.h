@@ -117,6 +117,9 @@ class Context {
   // diagnostic: 1 = the batched solver's scheduled run sees its first member's last error
   // above the stopping tolerance (0 = off)
   int inject_batch_err = 0;
+  // eigensolver: nodes of at least this size split with the Zolo-PD fast form (r = 8, every
+  // cost option), smaller ones with QDWH (batched per level); 0 = QDWH for every node
+  int eig_zolo_min = 4096;
   // batched solver: 1 = each bucket's iterations, H and unpacking run as one CUDA graph
   // launch from a host-computed schedule, 2 = the same launches issued eagerly, 0 = a
   // host-synchronized loop

@@ -78,21 +78,24 @@ double split_residual(Context& c, int n, int k, const double* H, int64_t ldh, co
                       int64_t lde) {
   const int64_t ldn = even(n);
   double* HV = c.buf("eig_hv", static_cast<size_t>(ldn) * n);
-  gemm(c, 0, 0, n, n, n, 1.0, Mat{const_cast<double*>(H), ldh, 0}, Mat{const_cast<double*>(V), ldv, 0}, 0.0,
-       Mat{HV, ldn, 0}, 1);
-  gemm(c, 1, 0, n, n, n, 1.0, Mat{const_cast<double*>(V), ldv, 0}, Mat{HV, ldn, 0}, 0.0, Mat{E, lde, 0}, 1);
+  {
+    OzScope mixed(c, c.zolo_mixed >= 1);  // normwise-accurate products in the mixed form
+    gemm(c, 0, 0, n, n, n, 1.0, Mat{const_cast<double*>(H), ldh, 0}, Mat{const_cast<double*>(V), ldv, 0}, 0.0,
+         Mat{HV, ldn, 0}, 1);
+    gemm(c, 1, 0, n, n, n, 1.0, Mat{const_cast<double*>(V), ldv, 0}, Mat{HV, ldn, 0}, 0.0, Mat{E, lde, 0}, 1);
+  }
   ck(frob2(n - k, k, E + k, lde, c.dpartial(), c.dscal() + 8, c.stream()));
   return std::sqrt(d2h(c, c.dscal() + 8));
 }
 
-// Runs task(ctx, i) for i in [0, count): on `c` itself for one task, otherwise on up to four
+// Runs task(ctx, i) for i in [0, count): on `c` itself for one task, otherwise on up to eight
 // worker contexts (own stream and workspace each, one host thread each) that take the tasks
 // in order.  Work queued on c.stream() before the call is visible to the tasks, and their work
 // is ordered before anything queued on c.stream() after it.  Rethrows a task's CUDA failure.
 template <class F>
 void run_concurrent(Context& c, int count, F&& task) {
   if (count <= 0) return;
-  const int W = std::min(count, 4);
+  const int W = std::min(count, 8);
   if (W == 1) {
     for (int i = 0; i < count; ++i) task(c, i);
     return;
@@ -110,6 +113,7 @@ void run_concurrent(Context& c, int count, F&& task) {
         ck(cudaStreamWaitEvent(wc.stream(), c.event(0), 0));
         wc.zolo_mixed = c.zolo_mixed;
         wc.oz_slices = c.oz_slices;
+        wc.eig_zolo_min = c.eig_zolo_min;
         for (int i = next++; i < count; i = next++) task(wc, i);
       } catch (const CudaFailure& e) {
         err[w] = e.err;
@@ -143,6 +147,30 @@ void split_candidates(const std::vector<double>& dg, double cand[4]) {
   cand[2] = med + 1e-3 * span;
   cand[3] = med - 1e-3 * span;
 }
+
+// The Zolo-PD fast form on a context for the scope (shared QR, Newton-Schulz finish,
+// explicit-inverse Cholesky, Frobenius beta, term plan; ||A||_F as alpha), restored on exit.
+struct FastForm {
+  Context& c;
+  int saved[6];
+  explicit FastForm(Context& ctx)
+      : c(ctx),
+        saved{ctx.zolo_shared_qr, ctx.zolo_ns_finish, ctx.zolo_chol_inverse, ctx.zolo_beta_frob, ctx.zolo_term_plan,
+              ctx.zolo_norm2} {
+    c.zolo_shared_qr = c.zolo_ns_finish = c.zolo_chol_inverse = c.zolo_beta_frob = c.zolo_term_plan = 1;
+    c.zolo_norm2 = 0;
+  }
+  ~FastForm() {
+    c.zolo_shared_qr = saved[0];
+    c.zolo_ns_finish = saved[1];
+    c.zolo_chol_inverse = saved[2];
+    c.zolo_beta_frob = saved[3];
+    c.zolo_term_plan = saved[4];
+    c.zolo_norm2 = saved[5];
+  }
+};
+
+bool zolo_node(const Context& c, int m) { return c.eig_zolo_min > 0 && m >= c.eig_zolo_min; }
 
 // The polar factor of H - sigma I for the first candidate shift, computed before the node is
 // split (the level's nodes in one batched solve): Up (ld even(m)), or info != 0 if it failed.
@@ -179,6 +207,22 @@ bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnor
     if (a == 0 && pre.Up) {
       if (pre.info != 0) continue;
       Ua = pre.Up;
+    } else if (a == 0 && zolo_node(c, m)) {
+      // a large node: the polar factor of H - sigma I by Zolo-PD (r = 8, fast form)
+      double* Hs = c.buf("eig_hs", static_cast<size_t>(ldm) * m);
+      ck(scale_copy(m, m, 1.0, nd.H, nd.ld, 0, Hs, ldm, 0, 1, 0.0, c.stream()));
+      ck(add_diag(m, Hs, ldm, -cand[0], c.stream()));
+      const Stats saved = c.stats;
+      int info;
+      {
+        FastForm ff(c);
+        info = zolo_polar(c, 8, m, m, Hs, ldm, Up, ldm, nullptr, 0);
+      }
+      S.zolo_calls++;
+      S.qdwh_iterations += c.stats.iterations;
+      S.flops += c.stats.flops;
+      c.stats = saved;
+      if (info != 0) continue;
     } else {
       QdwhOpts o;
       o.sym = 'N';
@@ -201,7 +245,10 @@ bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnor
     // subspace: V = full Q of QR(P * Omega); a second pass with X = P V1 if the split leaks
     double* Om = c.buf("eig_om", static_cast<size_t>(ldm) * k);
     ck(fill_random(m, k, Om, ldm, seed + a, c.stream()));
-    gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{Om, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
+    {
+      OzScope mixed(c, c.zolo_mixed >= 1);
+      gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{Om, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
+    }
     basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
     const double tol = 10.0 * eps * std::sqrt(static_cast<double>(m)) * std::max(hnorm, 1e-300);
     double off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
@@ -275,6 +322,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
           inner.push_back(i);
           tot += nodes[lo + i].n;
         }
+      // (the large nodes' Zolo-PD runs inside their split; the batch takes the others)
       double* dd = c.buf("eig_diag", std::max<size_t>(tot, 1));
       std::vector<double> hd(tot);
       size_t off = 0;
@@ -296,6 +344,10 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     // (zolo_qdwh_batch_dev's buckets and graphs; PQDWHFACS bounds per member)
     std::vector<Presolved> pre(cnt);
     double* arena = nullptr;
+    std::vector<int> small;
+    for (int i : inner)
+      if (!zolo_node(c, nodes[lo + i].n)) small.push_back(i);
+    inner.swap(small);
     if (inner.size() >= 2) {
       size_t tot = 0;
       for (int i : inner) tot += 2 * static_cast<size_t>(even(nodes[lo + i].n)) * nodes[lo + i].n;
@@ -342,6 +394,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     if (arena) mem.release(arena);
     for (int i = 0; i < cnt; ++i) {
       S.qdwh_calls += st[i].qdwh_calls;
+      S.zolo_calls += st[i].zolo_calls;
       S.qdwh_iterations += st[i].qdwh_iterations;
       S.subspace_passes += st[i].subspace_passes;
       S.splits += st[i].splits;
@@ -399,6 +452,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
       const Node& R = nodes[nd.right];
       const int m = nd.n, k = nd.k;
       const int64_t ldm = even(m);
+      OzScope mixed(wc, wc.zolo_mixed >= 1);
       gemm(wc, 0, 0, m, k, k, 1.0, Mat{nd.V, ldm, 0}, Mat{L.Z, even(L.n), 0}, 0.0, Mat{nd.Z, ldm, 0}, 1);
       gemm(wc, 0, 0, m, m - k, m - k, 1.0, Mat{nd.V + static_cast<int64_t>(k) * ldm, ldm, 0},
            Mat{R.Z, even(R.n), 0}, 0.0, Mat{nd.Z + static_cast<int64_t>(k) * ldm, ldm, 0}, 1);
@@ -500,7 +554,10 @@ int svd(Context& c, int m, int n, const double* dA, int64_t lda, int algo, int r
   const Stats pd = c.stats;
   info = syev_dc(c, n, H, ldn, dS, dV, ldv, es);
   if (info != 0) return info;
-  gemm(c, 0, 0, m, n, n, 1.0, Mat{Q, ldm, 0}, Mat{dV, ldv, 0}, 0.0, Mat{dU, ldu, 0}, 1);
+  {
+    OzScope mixed(c, c.zolo_mixed >= 1);
+    gemm(c, 0, 0, m, n, n, 1.0, Mat{Q, ldm, 0}, Mat{dV, ldv, 0}, 0.0, Mat{dU, ldu, 0}, 1);
+  }
   ck(cudaStreamSynchronize(c.stream()));
   c.stats = pd;
   return 0;

@@ -19,6 +19,7 @@ struct EigStats {
   double max_split_residual = 0.0;  // max ||V2^T H V1||_F / ||H||_F over the splits
   double flops = 0.0;
   int batched_nodes = 0;  // nodes whose first-candidate QDWH ran in a level's batched solve
+  int zolo_calls = 0;     // nodes whose first candidate's polar factor came from Zolo-PD
   // device ms (CUDA events on the calling stream): each top-down level's splits, the
   // Jacobi leaves, the bottom-up back-transformation, the whole call
   int levels = 0;
