@@ -11,6 +11,7 @@ namespace {
 constexpr int NB = kLeaf;  // leaf of the Cholesky / TRSM recursion
 constexpr int PW = 32;     // Householder panel width
 constexpr int QB = 128;    // Householder block: four panels, one rank-128 trailing update
+constexpr int QA = 512;    // reflector block of ormqr under the INT8-emulated GEMM: K = 512 updates
 
 int split_point(int n) {
   int n1 = ((n / 2) + NB - 1) / NB * NB;
@@ -336,8 +337,9 @@ static void panel_b_minus_vp(Context& c, const PanelRows& R, int jb, int ncols, 
 // blocks are the panels' T, and T_B(0:c0, q) = -T_B(0:c0, 0:c0) (V_B(:, 0:c0)^T V_q) T_q.
 // VB: the block's explicit V, mp packed rows.  T: the first panel's T (32 x 32 per panel).
 static void block_t(Context& c, int jb, Mat VB, int mp, const double* T, int64_t strideT, Mat TB, int batch) {
-  Mat G{c.buf("qr_bg", static_cast<size_t>(QB) * QB * batch), QB, static_cast<int64_t>(QB) * QB};
-  Mat Tmp{c.buf("qr_btmp", static_cast<size_t>(QB) * PW * batch), QB, static_cast<int64_t>(QB) * PW};
+  const int ldg = std::max(jb, 2);
+  Mat G{c.buf("qr_bg", static_cast<size_t>(ldg) * ldg * batch), ldg, static_cast<int64_t>(ldg) * ldg};
+  Mat Tmp{c.buf("qr_btmp", static_cast<size_t>(ldg) * PW * batch), ldg, static_cast<int64_t>(ldg) * PW};
   // lower triangle of V_B^T V_B: its transpose gives the blocks above the diagonal
   gemm(c, 1, 0, jb, jb, mp, 1.0, VB, VB, 0.0, G, batch, nullptr, 1, 0);
   ck(block_t_init(jb, T, strideT, TB.p, TB.ld, TB.stride, batch, c.stream()));
@@ -416,23 +418,28 @@ void geqrf(Context& c, int mtot, int n, int m_top, Mat W, double* tau, double* T
 // Q = H_1 ... H_k applied to the identity, one 128-column block reflector at a time from the
 // last block: Q(rows, J:nq) -= V_B (T_B (V_B^T Q(rows, J:nq))).  Columns left of J are still
 // identity columns with their one above the block's rows, so V_B^T leaves them zero.
-// C <- H_1 ... H_n C (the Q of geqrf applied from the left), one 128-column block reflector
-// at a time from the last: C(rows, cols) -= V_B (T_B (V_B^T C(rows, cols))).  from_diag: C
-// starts as the identity, so block J touches columns J .. ncols-1 only (left of J they are
-// identity columns with their one above the block's rows, which V_B^T leaves zero).
+// C <- H_1 ... H_n C (the Q of geqrf applied from the left), one block reflector of `width`
+// columns (a multiple of 32) at a time from the last: C(rows, cols) -= V_B (T_B (V_B^T
+// C(rows, cols))), T_B merged from the 32-column panels' T (block_t).  Width 128 gives K = 128
+// updates on the DMMA update tiles; 512 gives K = 512 products, which the INT8-emulated GEMM
+// takes (K >= 256), for about 1 % more flops in the T product; on DMMA both widths measure
+// the same.  from_diag: C starts as the identity, so block J touches columns J .. ncols-1 only
+// (left of J they are identity columns with their one above the block's rows, which V_B^T
+// leaves zero).
 static void apply_q_blocks(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat C, int ncols,
-                           bool from_diag, int batch, bool top_tri) {
+                           bool from_diag, int batch, bool top_tri, int width) {
   const int npan = (n + PW - 1) / PW;
   const int64_t ldv = (mtot + 1) / 2 * 2;
   const int64_t strideT = static_cast<int64_t>(npan) * PW * PW;
-  Mat VB{c.buf("qr_vb", static_cast<size_t>(ldv) * QB * batch), ldv, ldv * QB};
-  Mat TB{c.buf("qr_tb", static_cast<size_t>(QB) * QB * batch), QB, static_cast<int64_t>(QB) * QB};
-  Mat WB{c.buf("qr_wb", static_cast<size_t>(QB) * ncols * batch), QB, static_cast<int64_t>(QB) * ncols};
-  Mat PB{c.buf("qr_pb", static_cast<size_t>(QB) * ncols * batch), QB, static_cast<int64_t>(QB) * ncols};
-  const int nblk = (n + QB - 1) / QB;
+  const int bw = std::min(width, (n + PW - 1) / PW * PW);
+  Mat VB{c.buf("qr_vb", static_cast<size_t>(ldv) * bw * batch), ldv, ldv * bw};
+  Mat TB{c.buf("qr_tb", static_cast<size_t>(bw) * bw * batch), bw, static_cast<int64_t>(bw) * bw};
+  Mat WB{c.buf("qr_wb", static_cast<size_t>(bw) * ncols * batch), bw, static_cast<int64_t>(bw) * ncols};
+  Mat PB{c.buf("qr_pb", static_cast<size_t>(bw) * ncols * batch), bw, static_cast<int64_t>(bw) * ncols};
+  const int nblk = (n + bw - 1) / bw;
   for (int b = nblk - 1; b >= 0; --b) {
-    const int J = b * QB;
-    const int jbB = std::min(QB, n - J);
+    const int J = b * bw;
+    const int jbB = std::min(bw, n - J);
     const PanelRows R = panel_rows(mtot, m_top, top_tri, J, jbB);
     const int c0 = from_diag ? J : 0;
     const int nc = ncols - c0;
@@ -451,13 +458,13 @@ void orgqr(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat Q
   if (nq < n) nq = n;
   ck(set_identity(mtot, nq, Q.p, Q.ld, Q.stride, batch, 1.0, c.stream()));
   c.stats.launches++;
-  apply_q_blocks(c, mtot, n, m_top, W, T, Q, nq, true, batch, top_tri);
+  apply_q_blocks(c, mtot, n, m_top, W, T, Q, nq, true, batch, top_tri, QB);
 }
 
 void ormqr_left(Context& c, int mtot, int n, int m_top, Mat W, const double* T, Mat C, int ncols, int batch,
                 bool top_tri) {
   if (ncols <= 0) return;
-  apply_q_blocks(c, mtot, n, m_top, W, T, C, ncols, false, batch, top_tri);
+  apply_q_blocks(c, mtot, n, m_top, W, T, C, ncols, false, batch, top_tri, c.oz_active ? QA : QB);
 }
 
 }  // namespace zolo
