@@ -646,6 +646,11 @@ int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double*
     c.stats.terms[0] = es.qdwh_calls;
     c.stats.terms[1] = es.zolo_calls;
     c.stats.terms[2] = es.batched_nodes;
+    // host wall ms of the levels' phases (diagnostic): con[0..3]
+    c.stats.con[0] = es.wall_diag;
+    c.stats.con[1] = es.wall_batch;
+    c.stats.con[2] = es.wall_split;
+    c.stats.con[3] = es.wall_free;
     return info;
   });
 }

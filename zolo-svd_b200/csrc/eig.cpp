@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <mutex>
 #include <numeric>
@@ -21,6 +22,10 @@ namespace zolo {
 namespace {
 
 inline int64_t even(int64_t x) { return (x + 1) / 2 * 2; }
+
+double wall_ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
 
 struct DevMem {
   std::vector<void*> ptrs;
@@ -313,6 +318,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     std::vector<EigStats> st(cnt);
     std::vector<char> ok(cnt, 1);
     // the diagonals of the level's inner nodes (one read-back), their candidate shifts
+    auto w0 = std::chrono::steady_clock::now();
     std::vector<std::vector<double>> dg(cnt);
     std::vector<int> inner;
     {
@@ -342,6 +348,8 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     }
     // with two or more inner nodes, the QDWH of every node's H - sigma_0 I as one batched solve
     // (zolo_qdwh_batch_dev's buckets and graphs; PQDWHFACS bounds per member)
+    S.wall_diag += wall_ms_since(w0);
+    w0 = std::chrono::steady_clock::now();
     std::vector<Presolved> pre(cnt);
     double* arena = nullptr;
     std::vector<int> small;
@@ -387,10 +395,14 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
       S.flops += bs.flops_useful;
       S.batched_nodes += nb;
     }
+    S.wall_batch += wall_ms_since(w0);
+    w0 = std::chrono::steady_clock::now();
     run_concurrent(c, cnt, [&](Context& wc, int i) {
       ok[i] = split_node(wc, nodes[lo + i], kids[2 * i], kids[2 * i + 1], mem, hnorm,
                          0x5EEDull + (lo + i) * 7919ull, st[i], dg[i], pre[i]) ? 1 : 0;
     });
+    S.wall_split += wall_ms_since(w0);
+    w0 = std::chrono::steady_clock::now();
     if (arena) mem.release(arena);
     for (int i = 0; i < cnt; ++i) {
       S.qdwh_calls += st[i].qdwh_calls;
@@ -417,6 +429,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     // the split nodes' matrices are no longer needed (freed between levels: cudaFree waits)
     for (size_t i = lo; i < hi; ++i)
       if (i != 0 && !nodes[i].leaf) mem.release(nodes[i].H);
+    S.wall_free += wall_ms_since(w0);
     lo = hi;
   }
 

@@ -25,6 +25,9 @@ struct EigStats {
   int levels = 0;
   double ms_level[16] = {0};
   double ms_leaves = 0.0, ms_back = 0.0, ms_total = 0.0;
+  // host wall ms summed over the levels: diagonals read back, the batched QDWH solves, the
+  // concurrent splits, freeing the split nodes' matrices
+  double wall_diag = 0.0, wall_batch = 0.0, wall_split = 0.0, wall_free = 0.0;
 };
 
 // H = Z diag(w) Z^T for symmetric H (n x n); w ascending.  Returns 0 or > 0 on failure.
