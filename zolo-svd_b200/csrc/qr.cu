@@ -9,8 +9,11 @@
 // over independent rows and the row sums are 3 warp shuffles.  Column k costs
 // three CTA barriers and ONE cluster barrier:
 //   * gather: every CTA sums all CTAs' partials (||x_below||^2 and
-//     x_below . a_c) through distributed shared memory in the same fixed
-//     order, so all CTAs derive bit-identical beta / tau / v^T A;
+//     x_below . a_c) in the same fixed order, so all CTAs derive bit-identical
+//     beta / tau / v^T A; the partials were pushed into every CTA's receive
+//     slots (distributed shared memory stores) before the cluster barrier, so
+//     the sum reads local shared memory and the remote latency overlaps the
+//     barrier;
 //   * update: columns c > k apply reflector k;
 //   * scale + dots: column k is scaled into v_k and the partials of column
 //     k+1 are formed and published (double-buffered by column parity).
@@ -35,8 +38,7 @@ constexpr int NG = 8;    // row groups
 constexpr int UB = 8;    // rows per load batch
 constexpr int UC = 16;   // columns per load batch in the update
 constexpr int SLOT = 1 + QW;  // s0, d[QW]
-constexpr int ROWK = SLOT;    // pivot row of the next column follows the partials
-constexpr int SLOT_ALL = SLOT + QW;
+constexpr int QCL = 16;       // largest cluster
 constexpr size_t SMEM_CHUNK_CAP = 190 * 1024;
 
 struct PanelArgs {
@@ -61,7 +63,8 @@ ZDEV double group_sum8(double v) {
 }
 
 struct PanelShared {
-  double part[2][SLOT_ALL];
+  double recv[2][QCL][SLOT];  // partials of every CTA (by rank), double-buffered by column parity
+  double rowkr[2][QW];        // the pivot row of the next column, from the CTA holding it
   double sum[SLOT];
   double rowk[QW];
   double colk[QW];
@@ -132,35 +135,43 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
   }
   __syncthreads();
 
+  // partials into slot `slot` of receive buffer `bf` of every CTA of the cluster, the pivot
+  // row entry c likewise (stores to distributed shared memory, visible after the barrier)
+  auto publish = [&](int bf, int slot, double v) {
+    for (int q = 0; q < CL; ++q) *cluster.map_shared_rank(&S.recv[bf][rank][slot], q) = v;
+  };
+  auto publish_pivot = [&](int bf, int c, double v) {
+    for (int q = 0; q < CL; ++q) *cluster.map_shared_rank(&S.rowkr[bf][c], q) = v;
+  };
+
   // ---- partials of column 0 ----
   {
-    double acc = 0.0;
+    double acc = 0.0, pv = 0.0;
+    bool has_pv = false;
     if (col < w) {
       acc = dot_rows(first_row(1), 0);  // col 0: ||x_below||^2
-      if (r0 == 0 && grp == 0 && nloc > 0) S.part[0][ROWK + col] = at(0, col);  // pivot row 0
+      if (r0 == 0 && grp == 0 && nloc > 0) {  // pivot row 0
+        pv = at(0, col);
+        has_pv = true;
+      }
     }
     acc = group_sum8(acc);
-    if (grp == 0 && col < w) S.part[0][col == 0 ? 0 : 1 + col] = acc;
+    if (grp == 0 && col < w) publish(0, col == 0 ? 0 : 1 + col, acc);
+    if (has_pv) publish_pivot(0, col, pv);
   }
   cluster.sync();
 
   for (int k = 0; k < w; ++k) {
     const int buf = k & 1;
-    // ---- gather: thread i < SLOT sums entry i over all CTAs (same order everywhere) ----
+    // ---- gather: thread i < SLOT sums entry i over all CTAs in rank order (the same order
+    // everywhere) from this CTA's receive slots ----
     if (tid < SLOT) {
-      // all remote loads are issued before the first add (one DSMEM latency, not CL of them);
-      // the sum keeps the rank order
-      double v[16];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) v[q] = (q < CL) ? cluster.map_shared_rank(&S.part[buf][0], q)[tid] : 0.0;
       double s = 0.0;
-#pragma unroll
-      for (int q = 0; q < 16; ++q) s += v[q];
+      for (int q = 0; q < CL; ++q) s += S.recv[buf][q][tid];
       S.sum[tid] = s;
     } else if (tid < SLOT + w) {
-      const int owner = k / p.rows_per;
       const int c = tid - SLOT;
-      S.rowk[c] = cluster.map_shared_rank(&S.part[buf][0], owner)[ROWK + c];
+      S.rowk[c] = S.rowkr[buf][c];
     }
     __syncthreads();
 
@@ -228,14 +239,20 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
         V[r + k * ldv] = v;
       }
     }
-    double acc = 0.0;
+    double acc = 0.0, pv = 0.0;
+    bool has_pv = false;
     if (nk < w && col >= nk && col < w) {
       acc = dot_rows(first_row(nk + 1), nk);
       const int lr = nk - r0;  // pivot row of column k+1, if this CTA holds it
-      if (lr >= 0 && lr < nloc && grp == lr % NG) S.part[buf ^ 1][ROWK + col] = at(lr, col);
+      if (lr >= 0 && lr < nloc && grp == lr % NG) {
+        pv = at(lr, col);
+        has_pv = true;
+      }
     }
     acc = group_sum8(acc);
-    if (nk < w && grp == 0 && col >= nk && col < w) S.part[buf ^ 1][col == nk ? 0 : 1 + col] = acc;
+    // the other buffer: no CTA reads it before every CTA has passed this column's barrier
+    if (nk < w && grp == 0 && col >= nk && col < w) publish(buf ^ 1, col == nk ? 0 : 1 + col, acc);
+    if (has_pv) publish_pivot(buf ^ 1, col, pv);
     cluster.sync();
   }
 
