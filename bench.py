@@ -560,8 +560,11 @@ def run_gpu(args):
         return t, launches, last
 
     def profiled(form):
-        """per-kernel-class device time of one more solve (CUDA events around every launch)"""
-        h.profile(True)
+        """per-kernel-class device time of one more solve: CUDA events around every launch,
+        each launch timed alone (the device synchronized around it), the way a profiler's
+        serialized launch list times it, so that the look-ahead panels running beside the
+        trailing updates are not counted in the updates' time"""
+        h.profile(True, serialize=True)
         h.profile_read(reset=True)
         step(form, dA)
         torch.cuda.synchronize()
@@ -651,7 +654,9 @@ def run_gpu(args):
     g = {"ms": sum(prof[k]["ms"] for k in gk), "flops": sum(prof[k]["flops"] for k in gk),
          "launches": sum(prof[k]["launches"] for k in gk)}
     oz = prof.get("ozgemm", {"ms": 0.0, "flops": 0.0, "launches": 0})
-    prof_ms = sum(v["ms"] for v in prof.values())
+    # shares of the timed step (the profiled solve times each launch alone, like the
+    # serialized ncu launch list whose shares are relative to the solve's kernel time)
+    prof_ms = t_ms
     achieved = g["flops"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else 0.0
     per_class = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
                      "tflops": round(v["flops"] / (v["ms"] * 1e-3) / 1e12, 3) if v["ms"] > 0 else None}

@@ -86,7 +86,9 @@ const char* zolo_version(void);
  * triangle, 7 = FP64 product emulated on the INT8 tensor cores, 8 = GEMM with
  * 64 < K <= 256, class 0 then being K > 256).  While enabled, zolo_profile_read fills
  * out[3*cls + 0..2] = {launches, milliseconds, algorithmic flops} accumulated since the
- * last reset (out holds 27 doubles). */
+ * last reset (out holds 27 doubles).  on = 2 times every launch alone (the device is
+ * synchronized around it), as a profiler's serialized launch list does; on = 1 leaves the
+ * streams overlapping, so a launch's time includes work running beside it. */
 int zolo_profile_enable(zolo_handle_t handle, int on);
 /* Thread-block-cluster size the Householder panel kernel uses for an m x w panel on the
  * current device (negative when the rows do not fit in shared memory). */

@@ -445,8 +445,10 @@ class Handle:
             raise ZoloError(f"zolo_get_option({option})", rc)
         return v.value
 
-    def profile(self, on: bool = True):
-        lib().zolo_profile_enable(self.ptr, 1 if on else 0)
+    def profile(self, on: bool = True, serialize: bool = False):
+        """Per-kernel-class timing on (CUDA events around every launch); serialize: each launch
+        timed alone (device synchronized around it)."""
+        lib().zolo_profile_enable(self.ptr, (2 if serialize else 1) if on else 0)
 
     def profile_read(self, reset: bool = True) -> dict:
         """Per kernel class: launches, device ms (CUDA events) and algorithmic flops."""

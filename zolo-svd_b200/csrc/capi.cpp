@@ -323,6 +323,7 @@ int zolo_panel_cluster_size(int m, int w) { return zolo::qr_panel_config(m, w); 
 int zolo_profile_enable(zolo_handle_t h, int on) {
   return guarded(h, [&](Context& c) {
     c.prof.on = on != 0;
+    c.prof.serialize = on == 2;
     return 0;
   });
 }

@@ -112,6 +112,7 @@ cudaEvent_t Profiler::take() {
 }
 
 void Profiler::begin(int cls, double fl, cudaStream_t st, Rec* r) {
+  if (serialize) ck(cudaDeviceSynchronize());
   r->a = take();
   r->b = take();
   r->cls = cls;
@@ -122,6 +123,7 @@ void Profiler::begin(int cls, double fl, cudaStream_t st, Rec* r) {
 void Profiler::end(Rec& r, cudaStream_t st) {
   ck(cudaEventRecord(r.b, st));
   recs.push_back(r);
+  if (serialize) ck(cudaEventSynchronize(r.b));
 }
 
 void Profiler::collect() {

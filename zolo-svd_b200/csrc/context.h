@@ -44,6 +44,9 @@ struct Stats {
 struct Profiler {
   static constexpr int kClasses = 9;
   bool on = false;
+  // each launch timed alone: the device is synchronized before its first event, so that work
+  // overlapping on other streams (the look-ahead panels) is not counted in its time
+  bool serialize = false;
   struct Rec {
     cudaEvent_t a, b;
     int cls;

@@ -1070,6 +1070,11 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
     std::string key = "qdwh " + std::to_string(MB) + " " + std::to_string(NB) + " " + std::to_string(B) + " " +
                       (dH ? "h " : "- ") + (tail ? "t " : "- ");
     for (int k = 0; k < Ka; ++k) key += sqr[k] ? (gated[k] ? 'Q' : 'q') : (gated[k] ? 'C' : 'c');
+    // a bounded cache: a caller cycling through many bucket shapes keeps at most 256 graphs
+    if (c.graphs.size() >= 256 && c.graphs.find(key) == c.graphs.end()) {
+      ck(cudaStreamSynchronize(st));
+      c.drop_graphs();
+    }
     Context::CachedGraph& g = c.graphs[key];
     cudaGraphExec_t once = nullptr;  // a graph captured while the workspace grew: run once
     const bool capturable = c.batch_graph == 1 && !c.prof.on && st != cudaStreamLegacy && st != nullptr;
