@@ -83,10 +83,11 @@ const char* zolo_version(void);
 /* Per-kernel-class device timing with CUDA events on the launching streams
  * (0 = DMMA GEMM general shapes, 1 = Householder panel, 2 = Cholesky leaf,
  * 3 = GEMM M <= 32, 4 = GEMM N <= 64, 5 = GEMM rank-k K <= 64, 6 = GEMM lower
- * triangle, 7 = FP64 product emulated on the INT8 tensor cores, 8 = GEMM with
- * 64 < K <= 256, class 0 then being K > 256).  While enabled, zolo_profile_read fills
- * out[3*cls + 0..2] = {launches, milliseconds, algorithmic flops} accumulated since the
- * last reset (out holds 27 doubles).  on = 2 times every launch alone (the device is
+ * triangle, 7 = FP64 product emulated on the INT8 tensor cores (its INT8 kernel), 8 = GEMM
+ * with 64 < K <= 256, class 0 then being K > 256, 9 = the emulated products' splitting
+ * into digit planes).  While enabled, zolo_profile_read fills out[3*cls + 0..2] =
+ * {launches, milliseconds, algorithmic flops} accumulated since the last reset (out holds
+ * 30 doubles).  on = 2 times every launch alone (the device is
  * synchronized around it), as a profiler's serialized launch list does; on = 1 leaves the
  * streams overlapping, so a launch's time includes work running beside it. */
 int zolo_profile_enable(zolo_handle_t handle, int on);

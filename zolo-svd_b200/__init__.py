@@ -167,7 +167,7 @@ OPT_BATCH_GRAPH = 11
 OPT_INJECT_BATCH_ERR = 12
 OPT_EIG_ZOLO_MIN = 13
 PROFILE_CLASSES = ["dgemm", "qr_panel", "potrf_leaf", "dgemm_m32", "dgemm_n64", "dgemm_rank_k", "dgemm_tri",
-                   "ozgemm", "dgemm_k256"]
+                   "ozgemm", "dgemm_k256", "ozgemm_slicing"]
 
 EXPORTED = [s[0] for s in _SIGS] + ["pqdwhfacs_", "zolopd_", "pzolopd1_", "pzolopd2_", "zoloeig_"]
 

@@ -39,10 +39,11 @@ struct Stats {
 // their own stream: 0 = DMMA GEMM (general shapes, K > 64), 1 = Householder panel,
 // 2 = Cholesky leaf, 3 = GEMM with M <= 32, 4 = GEMM with N <= 64,
 // 5 = GEMM rank-k update (K <= 64), 6 = GEMM lower-triangle output, 7 = FP64 product
-// emulated on the INT8 tensor cores (ozgemm), 8 = GEMM with 64 < K <= 256 (the Householder
-// block-reflector updates); class 0 is then K > 256.
+// emulated on the INT8 tensor cores (the ozgemm kernel), 8 = GEMM with 64 < K <= 256 (the
+// Householder block-reflector updates; class 0 is then K > 256), 9 = the emulated
+// products' splitting into digit planes (row maxima and slices).
 struct Profiler {
-  static constexpr int kClasses = 9;
+  static constexpr int kClasses = 10;
   bool on = false;
   // each launch timed alone: the device is synchronized before its first event, so that work
   // overlapping on other streams (the look-ahead panels) is not counted in its time

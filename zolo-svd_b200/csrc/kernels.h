@@ -60,6 +60,9 @@ struct OzWork {
   int* expA = nullptr;
   int* expB = nullptr;
   int* status = nullptr;
+  // optional: recorded on the stream right before the INT8 kernel's launch (after the
+  // splitting), so that a caller can time the splitting and the kernel apart
+  cudaEvent_t before_kernel = nullptr, before_kernel2 = nullptr;
 };
 size_t ozgemm_work_bytes(const GemmArgs& a, int slices, OzWorkSizes* sz);
 bool ozgemm_k_ok(int slices, int K);

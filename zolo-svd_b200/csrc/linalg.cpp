@@ -163,13 +163,23 @@ void ozgemm(Context& c, int transA, int transB, int M, int N, int K, double alph
   w.expA = reinterpret_cast<int*>(rows + sz.rows_a + sz.rows_b);
   w.expB = w.expA + sz.rows_a;
   w.status = c.oz_status_word();
-  Profiler::Rec rec;
-  if (c.prof.on) {
-    const double f = algo_flops(M, N, K, tri, kfrom_n, kto_m);
-    c.prof.begin(7, f * batch, s, &rec);
+  // profiled: class 9 from the start to the kernel's launch (splitting), class 7 the kernel
+  Profiler::Rec split_rec, rec;
+  const bool profile = c.prof.on && M > 0 && N > 0 && K > 0 && batch > 0;  // the kernel runs
+  if (profile) {
+    c.prof.begin(9, 0.0, s, &split_rec);
+    rec.a = c.prof.take();
+    rec.b = c.prof.take();
+    rec.cls = 7;
+    rec.flops = algo_flops(M, N, K, tri, kfrom_n, kto_m) * batch;
+    w.before_kernel = split_rec.b;
+    w.before_kernel2 = rec.a;
   }
   ck(zolo::ozgemm(a, slices, w, s, num_sms()));
-  if (c.prof.on) c.prof.end(rec, s);
+  if (profile) {
+    c.prof.recs.push_back(split_rec);
+    c.prof.end(rec, s);
+  }
   c.stats.launches += 3;
 }
 

@@ -612,6 +612,11 @@ cudaError_t run(const GemmArgs& a, const OzWork& w, cudaStream_t st, int sms) {
   tiles *= a.batch;
   if (tiles <= 0 || tiles > 0x7fffffff) return cudaErrorInvalidValue;
   const int grid = static_cast<int>(std::min<int64_t>(tiles, sms));
+  if (w.before_kernel) {
+    e = cudaEventRecord(w.before_kernel, st);
+    if (e == cudaSuccess && w.before_kernel2) e = cudaEventRecord(w.before_kernel2, st);
+    if (e != cudaSuccess) return e;
+  }
   ozgemm_kernel<S><<<grid, kThreads, Cfg<S>::SMEM, st>>>(mapA, mapB, p);
   return cudaGetLastError();
 }
