@@ -1077,7 +1077,10 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
     }
     Context::CachedGraph& g = c.graphs[key];
     cudaGraphExec_t once = nullptr;  // a graph captured while the workspace grew: run once
-    const bool capturable = c.batch_graph == 1 && !c.prof.on && st != cudaStreamLegacy && st != nullptr;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ck(cudaStreamIsCapturing(st, &cap));
+    const bool capturable = c.batch_graph == 1 && !c.prof.on && st != cudaStreamLegacy && st != nullptr &&
+                            cap == cudaStreamCaptureStatusNone;
     if (capturable && g.seen) {
       if (g.exec && g.gen != c.alloc_gen()) {
         ck(cudaGraphExecDestroy(g.exec));
@@ -1233,12 +1236,11 @@ int qdwh_batch(Context& c, int count, const int* m, const int* n, const double* 
   const BucketPlan plan = plan_buckets(c.batch_model, count, m, n, kMaxBatch);
   const int nbk = static_cast<int>(plan.nb.size());
   const int W = std::min(std::max(1, c.batch_model.streams), nbk);
-  if (W <= 1) {
-    for (int b = 0; b < nbk; ++b)
-      qdwh_bucket(c, plan.members[b], plan.mb[b], plan.nb[b], m, n, dA, lda, dQ, ldq, dH, ldh, info, iterations, bs);
-  } else {
+  if (nbk > 0) {
     // the buckets are independent: spread them over W worker contexts (own stream and
-    // workspace each, driven by one host thread each) so that their launch chains overlap
+    // workspace each, driven by one host thread each) so that their launch chains overlap;
+    // a single bucket too runs on a worker's own stream, which its graph capture then holds
+    // alone (a capture of the caller's stream would take in other threads' work on it)
     while (static_cast<int>(c.workers.size()) < W) c.workers.emplace_back(new Context(c.device()));
     std::vector<int> order(nbk);
     for (int b = 0; b < nbk; ++b) order[b] = b;
@@ -1315,6 +1317,12 @@ int batch_autotune(Context& c) {
   const int sizes[3] = {64, 256, 1024};
   double lat[3], rate[3];
   double flops_at[3];
+  // the probes run on a worker context (own stream), as the solver's buckets do
+  if (c.workers.empty()) c.workers.emplace_back(new Context(c.device()));
+  Context& wc = *c.workers[0];
+  wc.batch_graph = c.batch_graph;
+  wc.inject_chol_fail = 0;
+  wc.inject_batch_err = 0;
   for (int k = 0; k < 3; ++k) {
     const int NB = sizes[k], MB = NB + NB / 2;
     std::vector<double> host(static_cast<size_t>(MB) * NB, 0.0);
@@ -1333,6 +1341,8 @@ int batch_autotune(Context& c) {
       pa[b] = dA + static_cast<size_t>(b) * MB * NB;
       pq[b] = dQ + static_cast<size_t>(b) * MB * NB;
     }
+    ck(cudaEventRecord(c.event(0), c.stream()));  // the probe inputs are on the device
+    ck(cudaStreamWaitEvent(wc.stream(), c.event(0), 0));
     double t[2];
     for (int rep = 0; rep < 2; ++rep) {
       const int nb_members = rep == 0 ? 1 : B;
@@ -1342,10 +1352,10 @@ int batch_autotune(Context& c) {
       // warm-up to the steady state the solver runs in: the first call sizes the workspace,
       // the second captures the bucket's graph (ZOLO_OPT_BATCH_GRAPH), the timed one replays it
       for (int w = 0; w < 2; ++w)
-        qdwh_bucket(c, idx, MB, NB, mm.data(), nn.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
+        qdwh_bucket(wc, idx, MB, NB, mm.data(), nn.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
                     nullptr, inf.data(), its.data(), &bs);
-      EventTimer tm(c.stream());
-      qdwh_bucket(c, idx, MB, NB, mm.data(), nn.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
+      EventTimer tm(wc.stream());
+      qdwh_bucket(wc, idx, MB, NB, mm.data(), nn.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
                   nullptr, inf.data(), its.data(), &bs);
       t[rep] = tm.stop();
     }
