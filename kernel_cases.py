@@ -21,6 +21,7 @@ solve (e.g. ``ncu -k regex:dgemm_kernel ... python kernel_cases.py --case gemm_n
   gemm_m512    the same on the DMMA GEMM
   polar        one Zolo-PD solve (bounds + PZOLOPD1 + H, zolo_polar_dev, FP64 fast form), kappa 1e12
   polar_mixed  the same in the mixed form (ZOLO_OPT_MIXED = 1)
+  batch        the 512-matrix batched QDWH (zolo_qdwh_batch_dev), bucket graphs replayed
 
   python kernel_cases.py --case gemm_nn --n 4096 --reps 3
 """
@@ -47,7 +48,7 @@ def load_pkg():
 
 
 CASES = ("gemm_nn", "gemm_rank32", "gemm_k128", "gemm_m32", "syrk", "geqrf", "potrf", "oz_nn", "oz_syrk", "oz_k128",
-         "oz_m512", "gemm_m512", "polar", "polar_mixed")
+         "oz_m512", "gemm_m512", "polar", "polar_mixed", "batch")
 
 
 def main() -> int:
@@ -150,6 +151,31 @@ def main() -> int:
                                      c.data_ptr(), n, tri, 0, args.slices)
             if rc:
                 raise zb.ZoloError("zolo_ozgemm_dev", rc)
+    elif args.case == "batch":
+        # the 512-member configuration's sizes (PCG64 seed 1004: n log-uniform in [64, 1024],
+        # m = n (1 + U[0,1]), kappa log-uniform in [1e2, 1e14], s geometric), the members built
+        # on the GPU from Haar factors; two calls first (eager, then captured), so that the
+        # timed calls replay the bucket graphs
+        import math
+        import numpy as np
+        rng = np.random.default_rng(1004)
+        mats = []
+        for _ in range(512):
+            nn = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+            mm = int(round(nn * (1 + rng.uniform(0, 1))))
+            kap = 10 ** rng.uniform(2, 14)
+            su = torch.from_numpy(np.geomspace(1.0, 1.0 / kap, nn)).to("cuda")
+            qu, ru = torch.linalg.qr(randn(mm, nn).T)
+            qv, rv = torch.linalg.qr(randn(nn, nn))
+            am = (qu * su[None, :]) @ qv.T  # m x n, row-major
+            mats.append((mm, nn, am.T.contiguous()))
+        outs = [(torch.empty_like(x), torch.empty((nn, nn), **f64)) for mm, nn, x in mats]
+        members = [(mm, nn, x.data_ptr(), mm, q.data_ptr(), mm, hq.data_ptr(), nn)
+                   for (mm, nn, x), (q, hq) in zip(mats, outs)]
+        zb.qdwh_batch_dev(h, members)
+
+        def run():
+            zb.qdwh_batch_dev(h, members)
     elif args.case == "geqrf":
         w0 = randn(n, n)
         w = torch.empty_like(w0)
@@ -186,6 +212,10 @@ def main() -> int:
         ms = e0.elapsed_time(e1)
         rate = f", {flops / (ms * 1e-3) / 1e12:.2f} TFLOP/s" if flops else ""
         print(f"{args.case} n={n} rep {i}: {ms:.3f} ms{rate}", flush=True)
+    if args.case == "batch":
+        st = zb.batch_stats(h)
+        print(f"batch: {h.stats()['launches']} kernel launches per call, {st['buckets']} buckets, "
+              f"{st['graph_replays']} graph replays", flush=True)
     h.close()
     return 0
 
