@@ -78,16 +78,18 @@ void basis_from(Context& c, int n, int k, Mat X, double* V, int64_t ldv) {
   orgqr(c, n, k, -1, X, T, Mat{V, ldv, 0}, 1, n);
 }
 
-// off = ||E(k:n, 0:k)||_F for E = V^T H V (E returned)
+// off = ||E(k:n, 0:k)||_F for E = V^T H V, returned in E; lower_only: only its lower triangle
+// is formed (E is symmetric, and a split needs the diagonal blocks and the block below them)
 double split_residual(Context& c, int n, int k, const double* H, int64_t ldh, const double* V, int64_t ldv, double* E,
-                      int64_t lde) {
+                      int64_t lde, bool lower_only) {
   const int64_t ldn = even(n);
   double* HV = c.buf("eig_hv", static_cast<size_t>(ldn) * n);
   {
     OzScope mixed(c, c.zolo_mixed >= 1);  // normwise-accurate products in the mixed form
     gemm(c, 0, 0, n, n, n, 1.0, Mat{const_cast<double*>(H), ldh, 0}, Mat{const_cast<double*>(V), ldv, 0}, 0.0,
          Mat{HV, ldn, 0}, 1);
-    gemm(c, 1, 0, n, n, n, 1.0, Mat{const_cast<double*>(V), ldv, 0}, Mat{HV, ldn, 0}, 0.0, Mat{E, lde, 0}, 1);
+    gemm(c, 1, 0, n, n, n, 1.0, Mat{const_cast<double*>(V), ldv, 0}, Mat{HV, ldn, 0}, 0.0, Mat{E, lde, 0}, 1,
+         nullptr, lower_only ? 1 : 0);
   }
   ck(frob2(n - k, k, E + k, lde, c.dpartial(), c.dscal() + 8, c.stream()));
   return std::sqrt(d2h(c, c.dscal() + 8));
@@ -256,12 +258,12 @@ bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnor
     }
     basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
     const double tol = 10.0 * eps * std::sqrt(static_cast<double>(m)) * std::max(hnorm, 1e-300);
-    double off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
+    double off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm, true);
     S.subspace_passes++;
     for (int pass = 1; pass < 3 && off > tol; ++pass) {
       gemm(c, 0, 0, m, k, m, 1.0, Mat{P, ldm, 0}, Mat{nd.V, ldm, 0}, 0.0, Mat{X, ldm, 0}, 1);
       basis_from(c, m, k, Mat{X, ldm, 0}, nd.V, ldm);
-      off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm);
+      off = split_residual(c, m, k, nd.H, nd.ld, nd.V, ldm, E, ldm, true);
       S.subspace_passes++;
     }
     S.max_split_residual = std::max(S.max_split_residual, off / std::max(hnorm, 1e-300));
@@ -272,13 +274,13 @@ bool split_node(Context& c, Node& nd, Node& L, Node& R, DevMem& mem, double hnor
     L.ld = even(k);
     L.H = mem.alloc(static_cast<size_t>(L.ld) * k);
     ck(scale_copy(k, k, 1.0, E, ldm, 0, L.H, L.ld, 0, 1, 0.0, c.stream()));
-    ck(symmetrize(k, L.H, L.ld, c.stream()));
+    ck(mirror_lower(k, L.H, L.ld, c.stream()));
     R.n = m - k;
     R.ld = even(m - k);
     R.H = mem.alloc(static_cast<size_t>(R.ld) * (m - k));
     ck(scale_copy(m - k, m - k, 1.0, E + k + static_cast<int64_t>(k) * ldm, ldm, 0, R.H, R.ld, 0, 1, 0.0,
                   c.stream()));
-    ck(symmetrize(m - k, R.H, R.ld, c.stream()));
+    ck(mirror_lower(m - k, R.H, R.ld, c.stream()));
     S.splits++;
     return true;
   }
@@ -529,7 +531,7 @@ int zoloeig(Context& c, int n, const double* dQ, int64_t ldq, const double* dA, 
     orgqr(c, n, kk, -1, Mat{X, ldn, 0}, T, Mat{Y, ldn, 0}, 1, kk);
     gemm(c, 0, 0, n, kk, n, 1.0, Mat{C, ldn, 0}, Mat{Y, ldn, 0}, 0.0, Mat{X, ldn, 0}, 1);
     basis_from(c, n, kk, Mat{X, ldn, 0}, V, ldvv);
-    const double off = split_residual(c, n, rk, dA, lda, V, ldvv, E, ldee) / norma;
+    const double off = split_residual(c, n, rk, dA, lda, V, ldvv, E, ldee, false) / norma;
     // err is the leading-rows block of the reference (E(1:Rk, Rk+1:N)); E is symmetric here
     if (off <= 4.0 * tol1 || it == 2) break;
     ck(scale_copy(n, rk, 1.0, V, ldvv, 0, Y, ldn, 0, 1, 0.0, c.stream()));

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <thread>
 #include <vector>
@@ -1079,7 +1080,11 @@ void qdwh_bucket(Context& c, const std::vector<int>& idx, int MB, int NB, const 
     cudaGraphExec_t once = nullptr;  // a graph captured while the workspace grew: run once
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     ck(cudaStreamIsCapturing(st, &cap));
-    const bool capturable = c.batch_graph == 1 && !c.prof.on && st != cudaStreamLegacy && st != nullptr &&
+    // no capture under an injected CUDA tool (a profiler sets CUDA_INJECTION64_PATH): the
+    // worker threads' concurrent captures ended the process under one; the same schedule then
+    // runs eagerly
+    static const bool tool = std::getenv("CUDA_INJECTION64_PATH") != nullptr;
+    const bool capturable = c.batch_graph == 1 && !c.prof.on && !tool && st != cudaStreamLegacy && st != nullptr &&
                             cap == cudaStreamCaptureStatusNone;
     if (capturable && g.seen) {
       if (g.exec && g.gen != c.alloc_gen()) {
