@@ -654,6 +654,11 @@ def run_gpu(args):
     g = {"ms": sum(prof[k]["ms"] for k in gk), "flops": sum(prof[k]["flops"] for k in gk),
          "launches": sum(prof[k]["launches"] for k in gk)}
     oz = prof.get("ozgemm", {"ms": 0.0, "flops": 0.0, "launches": 0})
+    # the same DMMA roofline in the plain FP64 form, where DMMA carries every product
+    gk64 = [k for k in prof_fp64 if k.startswith("dgemm")]
+    g64 = {"ms": sum(prof_fp64[k]["ms"] for k in gk64), "flops": sum(prof_fp64[k]["flops"] for k in gk64),
+           "launches": sum(prof_fp64[k]["launches"] for k in gk64)}
+    ach64 = g64["flops"] / (g64["ms"] * 1e-3) / 1e12 if g64["ms"] > 0 else 0.0
     # shares of the timed step (the profiled solve times each launch alone, like the
     # serialized ncu launch list whose shares are relative to the solve's kernel time)
     prof_ms = t_ms
@@ -707,6 +712,11 @@ def run_gpu(args):
                          "traffic": DGEMM_TRAFFIC_BYTES, "traffic_launch": DGEMM_TRAFFIC_LAUNCH,
                          "share_of_step": g["ms"] / prof_ms if prof_ms else None,
                          "launches_per_step": g["launches"]},
+            "roofline_fp64_form": {"bound": "tensor", "kernel": "dgemm_kernel (all shapes) in the plain FP64 form",
+                                   "achieved": ach64, "peak": peak, "unit": "TFLOP/s",
+                                   "frac": ach64 / peak if peak else None,
+                                   "share_of_step": g64["ms"] / t_fp64 if t_fp64 else None,
+                                   "launches_per_step": g64["launches"]},
             "roofline_ozgemm": {"bound": "tensor", "kernel": "ozgemm_kernel<8> (INT8 tcgen05.mma kind::i8, TMA, "
                                                              "TMEM accumulators)",
                                 "achieved": oz_tops, "peak": i8_peak, "unit": "TOP/s (int8)",
