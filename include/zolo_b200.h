@@ -369,8 +369,8 @@ int zolo_form_h_dev(zolo_handle_t h, int m, int n, const double* dQ, int64_t ldq
  * zolo_get_stats afterwards: iterations = splits, qr_iterations = QDWH iterations,
  * chol_iterations = leaves, last_err = largest split residual / ||H||_F, ms_step[l] = device
  * ms of top-down level l, ms_finish = the leaves, ms_h = the back-transformation,
- * ns_steps = subspace passes, terms[0..2] = QDWH solves, Zolo-PD solves, nodes solved in
- * a level's batched QDWH, con[0..3] = host wall ms summed over the levels of reading the
+ * ns_steps = subspace passes, terms[0..3] = QDWH solves, Zolo-PD solves, nodes solved in
+ * a level's batched QDWH, workspace buffers grown during the call, con[0..3] = host wall ms summed over the levels of reading the
  * diagonals, the batched QDWH solves, the concurrent splits and freeing split nodes. */
 int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double* dW, double* dZ, int64_t ldz);
 /* Zolo-SVD (test_zolodrv1.f90 + ZoloCHK1.f90:80-91): A = U diag(s) V^T for m >= n via

@@ -51,7 +51,9 @@ int guarded(zolo_handle_t h, F&& f) {
   std::lock_guard<std::mutex> lk(h->ctx.mu);
   try {
     DeviceGuard dg(h->ctx.device());
-    return f(h->ctx);
+    const int r = f(h->ctx);
+    h->ctx.sync_and_free_retired();  // blocks replaced while the call ran
+    return r;
   } catch (const CudaFailure& e) {
     return kCudaBase - static_cast<int>(e.err);
   } catch (const std::bad_alloc&) {
@@ -647,6 +649,7 @@ int zolo_syev_dev(zolo_handle_t h, int n, const double* dH, int64_t ldh, double*
     c.stats.terms[0] = es.qdwh_calls;
     c.stats.terms[1] = es.zolo_calls;
     c.stats.terms[2] = es.batched_nodes;
+    c.stats.terms[3] = static_cast<int>(es.reallocs);
     // host wall ms of the levels' phases (diagnostic): con[0..3]
     c.stats.con[0] = es.wall_diag;
     c.stats.con[1] = es.wall_batch;

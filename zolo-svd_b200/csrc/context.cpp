@@ -35,6 +35,53 @@ void Context::free_retired() {
   retired_.clear();
 }
 
+void* Context::pool_take(size_t bytes, size_t* got) {
+  {
+    std::lock_guard<std::mutex> lk(pool_mu_);
+    auto it = pool_.lower_bound(bytes);
+    if (it != pool_.end() && it->first <= 2 * bytes) {
+      void* p = it->second;
+      *got = it->first;
+      pool_.erase(it);
+      return p;
+    }
+  }
+  const size_t b = (bytes + 65535) / 65536 * 65536;
+  void* p = nullptr;
+  ck(cudaMalloc(&p, b));
+  *got = b;
+  return p;
+}
+
+void Context::pool_give(void* p, size_t bytes) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(pool_mu_);
+  pool_.emplace(bytes, p);
+}
+
+void Context::sync_all() {
+  cudaStreamSynchronize(stream_);
+  cudaStreamSynchronize(side_);
+  for (auto& w : workers) {
+    cudaStreamSynchronize(w->stream_);
+    cudaStreamSynchronize(w->side_);
+  }
+}
+
+void Context::sync_and_free_retired() {
+  bool any = !retired_.empty();
+  for (auto& w : workers) any = any || !w->retired_.empty();
+  if (!any) return;
+  ck(cudaStreamSynchronize(stream_));
+  ck(cudaStreamSynchronize(side_));
+  for (auto& w : workers) {
+    ck(cudaStreamSynchronize(w->stream_));
+    ck(cudaStreamSynchronize(w->side_));
+    w->free_retired();
+  }
+  free_retired();
+}
+
 void Context::release_all() {
   workers.clear();
   if (stream_) cudaStreamSynchronize(stream_);
@@ -43,6 +90,11 @@ void Context::release_all() {
   free_retired();
   for (auto& kv : bufs_) cudaFree(kv.second.first);
   bufs_.clear();
+  {
+    std::lock_guard<std::mutex> lk(pool_mu_);
+    for (auto& kv : pool_) cudaFree(kv.second);
+    pool_.clear();
+  }
   ++alloc_gen_;
   if (splitk_.ptr) cudaFree(splitk_.ptr);
   if (splitk_side_.ptr) cudaFree(splitk_side_.ptr);
@@ -54,15 +106,14 @@ void* Context::grow(const std::string& name, size_t bytes) {
   auto it = bufs_.find(name);
   if (it != bufs_.end() && it->second.second >= bytes) return it->second.first;
   if (it != bufs_.end()) {
-    if (capturing) {
-      retired_.push_back(it->second.first);  // captured nodes may reference the old block
-    } else {
-      // kernels queued on the stream may still use the old block
-      ck(cudaStreamSynchronize(stream_));
-      ck(cudaFree(it->second.first));
-    }
+    // kernels queued on this context's streams (or captured nodes) may still use the old
+    // block: it is kept alive and freed once they have run (free_retired after a
+    // synchronization), instead of a cudaFree here, which would wait for the whole device
+    // while other worker contexts are running
+    retired_.push_back(it->second.first);
     bufs_.erase(it);
     ++alloc_gen_;
+    ++reallocs;
   }
   void* p = nullptr;
   const size_t b = bytes < 256 ? 256 : bytes;
@@ -83,14 +134,9 @@ void Context::ensure_splitk(size_t bytes, bool side) {
   Scratch& s = side ? splitk_side_ : splitk_;
   if (s.bytes >= bytes) return;
   if (s.ptr) {
-    if (capturing) {
-      retired_.push_back(s.ptr);
-    } else {
-      ck(cudaStreamSynchronize(stream_));
-      ck(cudaStreamSynchronize(side_));
-      ck(cudaFree(s.ptr));
-    }
+    retired_.push_back(s.ptr);  // freed by free_retired, as in grow
     ++alloc_gen_;
+    ++reallocs;
   }
   s.ptr = nullptr;
   s.bytes = 0;

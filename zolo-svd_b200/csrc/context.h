@@ -136,13 +136,23 @@ class Context {
   // digit planes of the products gemm() routes to ozgemm right now (0 = none); set by OzScope
   int oz_active = 0;
 
-  // Stream capture: while `capturing`, a buffer that must grow is replaced without a
-  // synchronization and the old block is kept alive (retired) until free_retired(), after
-  // the captured work has run.  alloc_gen changes whenever a block that captured work may
-  // reference is replaced or freed, which invalidates cached graphs.
+  // A buffer that must grow is replaced without a synchronization and the old block is kept
+  // alive (retired) until free_retired(), called once the work that may use it has run (the
+  // end of a bucket's solve, or sync_and_free_retired() after a library call, which also
+  // covers the worker contexts).  alloc_gen changes whenever a block is replaced or freed,
+  // which invalidates cached graphs; `capturing` marks a stream capture in progress.
   bool capturing = false;
   uint64_t alloc_gen() const { return alloc_gen_; }
   void free_retired();
+  void sync_and_free_retired();
+  // waits for this context's and its workers' streams (errors ignored: used on exit paths)
+  void sync_all();
+  // Pool of device blocks for call-scoped matrices (the eigensolver's nodes): pool_take returns
+  // a free block of at least `bytes` (and at most twice that) or a new one, its size in *got;
+  // pool_give puts it back.  Blocks are freed by release_all only.  Thread-safe.
+  void* pool_take(size_t bytes, size_t* got);
+  void pool_give(void* p, size_t bytes);
+  int64_t reallocs = 0;  // buffers replaced by larger ones (diagnostic)
   // cached executable graphs of the batched solver, by bucket shape and schedule
   struct CachedGraph {
     cudaGraphExec_t exec = nullptr;
@@ -166,6 +176,8 @@ class Context {
   std::map<std::string, std::pair<void*, size_t>> bufs_;
   Scratch splitk_, splitk_side_;
   std::vector<void*> retired_;
+  std::multimap<size_t, void*> pool_;
+  std::mutex pool_mu_;
   uint64_t alloc_gen_ = 0;
   void* grow(const std::string& name, size_t bytes);
 };

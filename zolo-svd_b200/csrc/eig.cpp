@@ -27,26 +27,36 @@ double wall_ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// The divide-and-conquer's node matrices: blocks from the handle's pool (reused across calls,
+// cudaMalloc only when no free block fits), returned to it when released.  A block released
+// between levels is reused by a later level's work only, which runs on streams ordered after
+// the releasing level's (each level's workers wait for the previous level's).
 struct DevMem {
-  std::vector<void*> ptrs;
+  Context& pool;
+  std::vector<std::pair<void*, size_t>> blocks;
   std::mutex mu;  // nodes of one level are split by concurrent workers
+  explicit DevMem(Context& c) : pool(c) {}
   double* alloc(size_t elems) {
-    void* p = nullptr;
-    ck(cudaMalloc(&p, std::max<size_t>(elems, 1) * sizeof(double)));
     std::lock_guard<std::mutex> lk(mu);
-    ptrs.push_back(p);
+    size_t bytes = 0;
+    void* p = pool.pool_take(std::max<size_t>(elems, 1) * sizeof(double), &bytes);
+    blocks.emplace_back(p, bytes);
     return static_cast<double*>(p);
   }
   void release(double* p) {
-    for (auto& q : ptrs)
-      if (q == p) {
-        cudaFree(q);
-        q = nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& b : blocks)
+      if (b.first == p) {
+        pool.pool_give(b.first, b.second);
+        b.first = nullptr;
       }
   }
+  // every block back to the pool once the work queued on the handle's and the workers'
+  // streams has run (also on an error return)
   ~DevMem() {
-    for (void* p : ptrs)
-      if (p) cudaFree(p);
+    pool.sync_all();
+    for (auto& b : blocks)
+      if (b.first) pool.pool_give(b.first, b.second);
   }
 };
 
@@ -99,8 +109,11 @@ double split_residual(Context& c, int n, int k, const double* H, int64_t ldh, co
 // worker contexts (own stream and workspace each, one host thread each) that take the tasks
 // in order.  Work queued on c.stream() before the call is visible to the tasks, and their work
 // is ordered before anything queued on c.stream() after it.  Rethrows a task's CUDA failure.
+// The tasks go to the workers by a fixed rule, the costliest first onto the least loaded
+// worker (cost[i] estimates task i), so that the same nodes meet the same worker and its
+// workspace on every call with the same split sizes.
 template <class F>
-void run_concurrent(Context& c, int count, F&& task) {
+void run_concurrent(Context& c, int count, const std::vector<double>& cost, F&& task) {
   if (count <= 0) return;
   const int W = std::min(count, 8);
   if (W == 1) {
@@ -108,8 +121,18 @@ void run_concurrent(Context& c, int count, F&& task) {
     return;
   }
   while (static_cast<int>(c.workers.size()) < W) c.workers.emplace_back(new Context(c.device()));
+  std::vector<int> order(count);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<std::vector<int>> assign(W);
+  std::vector<double> load(W, 0.0);
+  for (int i : order) {
+    const int w = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+    assign[w].push_back(i);
+    load[w] += cost[i] + 1.0;
+  }
   ck(cudaEventRecord(c.event(0), c.stream()));
-  std::atomic<int> next{0};
+  std::atomic<bool> stop{false};
   std::vector<cudaError_t> err(W, cudaSuccess);
   std::vector<std::thread> th;
   for (int w = 0; w < W; ++w) {
@@ -121,13 +144,16 @@ void run_concurrent(Context& c, int count, F&& task) {
         wc.zolo_mixed = c.zolo_mixed;
         wc.oz_slices = c.oz_slices;
         wc.eig_zolo_min = c.eig_zolo_min;
-        for (int i = next++; i < count; i = next++) task(wc, i);
+        for (int i : assign[w]) {
+          if (stop) break;
+          task(wc, i);
+        }
       } catch (const CudaFailure& e) {
         err[w] = e.err;
-        next = count;
+        stop = true;
       } catch (...) {
         err[w] = cudaErrorUnknown;
-        next = count;
+        stop = true;
       }
     });
   }
@@ -294,8 +320,14 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   EigStats local;
   EigStats& S = es ? *es : local;
   S = EigStats{};
+  auto reallocs_now = [&]() {
+    int64_t r = c.reallocs;
+    for (auto& w : c.workers) r += w->reallocs;
+    return r;
+  };
+  const int64_t reallocs0 = reallocs_now();
   EventTimer total(c.stream());
-  DevMem mem;
+  DevMem mem(c);
   std::vector<Node> nodes;
   {
     Node root;
@@ -385,8 +417,20 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
       }
       BatchStats bs;
       const Stats saved = c.stats;
-      const int rb = qdwh_batch(c, nb, mm.data(), mm.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr,
-                                nullptr, inf.data(), its.data(), &bs);
+      // the schedule issued eagerly: the split sizes, and with them the bucket shapes, rarely
+      // recur, so a captured graph would be replayed seldom and its capture costs more than it
+      // saves
+      const int saved_graph = c.batch_graph;
+      if (c.batch_graph == 1) c.batch_graph = 2;
+      int rb = -1;
+      try {
+        rb = qdwh_batch(c, nb, mm.data(), mm.data(), pa.data(), ld.data(), pq.data(), ld.data(), nullptr, nullptr,
+                        inf.data(), its.data(), &bs);
+      } catch (...) {
+        c.batch_graph = saved_graph;
+        throw;
+      }
+      c.batch_graph = saved_graph;
       c.stats = saved;
       if (rb != 0) std::fill(inf.begin(), inf.end(), 1);  // each node then solves on its own
       S.qdwh_calls += nb;
@@ -399,7 +443,9 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
     }
     S.wall_batch += wall_ms_since(w0);
     w0 = std::chrono::steady_clock::now();
-    run_concurrent(c, cnt, [&](Context& wc, int i) {
+    std::vector<double> cost(cnt);
+    for (int i = 0; i < cnt; ++i) cost[i] = std::pow(static_cast<double>(nodes[lo + i].n), 3);
+    run_concurrent(c, cnt, cost, [&](Context& wc, int i) {
       ok[i] = split_node(wc, nodes[lo + i], kids[2 * i], kids[2 * i + 1], mem, hnorm,
                          0x5EEDull + (lo + i) * 7919ull, st[i], dg[i], pre[i]) ? 1 : 0;
     });
@@ -442,9 +488,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   S.leaves = static_cast<int>(leaves.size());
   EventTimer tleaf(c.stream());
   {
-    void* dl = nullptr;
-    ck(cudaMalloc(&dl, sizeof(JacobiLeaf) * leaves.size()));
-    mem.ptrs.push_back(dl);
+    void* dl = mem.alloc((sizeof(JacobiLeaf) * leaves.size() + sizeof(double) - 1) / sizeof(double));
     int* dsw = c.ibuf("eig_sweeps", leaves.size());
     ck(cudaMemcpyAsync(dl, leaves.data(), sizeof(JacobiLeaf) * leaves.size(), cudaMemcpyHostToDevice, c.stream()));
     ck(jacobi_leaves(static_cast<JacobiLeaf*>(dl), static_cast<int>(leaves.size()), 30, dsw, c.stream()));
@@ -460,7 +504,9 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   for (auto lv = levels.rbegin(); lv != levels.rend(); ++lv) {
     const size_t lo = lv->first;
     const int cnt = static_cast<int>(lv->second - lv->first);
-    run_concurrent(c, cnt, [&](Context& wc, int i) {
+    std::vector<double> cost(cnt);
+    for (int i = 0; i < cnt; ++i) cost[i] = nodes[lo + i].leaf ? 0.0 : std::pow(static_cast<double>(nodes[lo + i].n), 3);
+    run_concurrent(c, cnt, cost, [&](Context& wc, int i) {
       Node& nd = nodes[lo + i];
       if (nd.leaf) return;
       const Node& L = nodes[nd.left];
@@ -497,6 +543,7 @@ int syev_dc(Context& c, int n, const double* dH, int64_t ldh, double* dW, double
   ck(cudaMemcpyAsync(dW, ws.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c.stream()));
   ck(gather_columns(n, n, root.Z, even(n), dperm, dZ, ldz, c.stream()));
   S.ms_total = total.stop();
+  S.reallocs = reallocs_now() - reallocs0;
   return 0;
 }
 

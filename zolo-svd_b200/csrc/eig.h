@@ -20,6 +20,7 @@ struct EigStats {
   double flops = 0.0;
   int batched_nodes = 0;  // nodes whose first-candidate QDWH ran in a level's batched solve
   int zolo_calls = 0;     // nodes whose first candidate's polar factor came from Zolo-PD
+  int64_t reallocs = 0;   // workspace buffers replaced by larger ones during the call
   // device ms (CUDA events on the calling stream): each top-down level's splits, the
   // Jacobi leaves, the bottom-up back-transformation, the whole call
   int levels = 0;
