@@ -7,7 +7,7 @@
 // work is column-parallel: thread (c, g) owns column c of the rows
 // r = g, g+8, g+16, ... of its chunk, so every phase is a short scalar loop
 // over independent rows and the row sums are 3 warp shuffles.  Column k costs
-// two CTA barriers and ONE cluster barrier:
+// three CTA barriers and ONE cluster barrier:
 //   * gather: every CTA sums all CTAs' partials (||x_below||^2 and
 //     x_below . a_c) in the same fixed order, so all CTAs derive bit-identical
 //     beta / tau / v^T A; the partials were pushed into every CTA's receive
@@ -67,6 +67,7 @@ struct PanelShared {
   double rowkr[2][QW];        // the pivot row of the next column, from the CTA holding it
   double sum[SLOT];
   double rowk[QW];
+  double colk[QW];
   double tauv[QW];
   double G[QW * QW];   // this CTA's partial V^T V (upper triangle)
   double Gs[QW * QW];  // rank 0: cluster sum of G
@@ -187,16 +188,16 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
       tau = (beta - alpha) / beta;
       scal = 1.0 / (alpha - beta);
     }
+    if (tid < w) S.colk[tid] = (tid > k) ? S.rowk[tid] + scal * S.sum[1 + tid] : 0.0;  // v^T a_c
     if (tid == 0) {
-      S.tauv[k] = tau;  // read after the loop only
+      S.tauv[k] = tau;
       if (rank == 0) p.tau[b * p.strideTau + k] = tau;
     }
+    __syncthreads();
 
     // ---- update: a(r,c) -= tau * v_r * (v^T a_c) for c > k, rows r >= k ----
-    // v^T a_c = a(k,c) + scal * x_below . a_c from the gathered sums, formed by every thread
-    // for the columns it updates (the same expression everywhere, so no barrier is needed to
-    // share it); each thread owns whole rows and loads a batch of UC columns before storing
-    // any (a store may alias the next loads of the same array, so batching is explicit)
+    // each thread owns whole rows and loads a batch of UC columns before storing any
+    // (a store may alias the next loads of the same array, so batching is explicit)
     for (int rl = max(k - r0, 0) + tid; rl < nloc; rl += QT) {
       const double tv = tau * ((r0 + rl == k) ? 1.0 : at(rl, k) * scal);
       for (int c0 = k + 1; c0 < w; c0 += UC) {
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(QT) qr_panel_kernel(PanelArgs p) {
           if (c0 + u < w) xc[u] = at(rl, c0 + u);
 #pragma unroll
         for (int u = 0; u < UC; ++u)
-          if (c0 + u < w) at(rl, c0 + u) = xc[u] - tv * (S.rowk[c0 + u] + scal * S.sum[1 + c0 + u]);
+          if (c0 + u < w) at(rl, c0 + u) = xc[u] - tv * S.colk[c0 + u];
       }
     }
     __syncthreads();
