@@ -109,7 +109,9 @@ int zolo_profile_read(zolo_handle_t handle, double* out, int reset);
  * FP64 Newton-Schulz steps X <- X (3I - X^T X)/2 instead of further Zolo
  * iterations, re-measuring e before each step and stopping at rounding level
  * (max(1e-14, eps sqrt(m)/2), or when a step no longer halves e; at most 12 steps,
- * none when e is already there).  The polar factor of X is that of A, so the result
+ * none when e is already there; the Gram after a step is not formed when the step's bound on
+ * the next e, 3/4 e^2 sqrt(n) (1 + e sqrt(n)/3), is below a tenth of that level).  The polar
+ * factor of X is that of A, so the result
  * agrees with the reference rule's to rounding.  With this option the loop ends at that
  * measured check rather than on ||X_{k+1} - X_k||.  No reference counterpart. */
 #define ZOLO_OPT_NS_FINISH 2

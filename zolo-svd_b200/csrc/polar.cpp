@@ -220,7 +220,8 @@ void zolo_terms_shared_qr(Context& c, int m, int n, const double* X, int64_t ldx
 // Finish of the polar iteration by FP64 Newton-Schulz steps X <- X (3I - X^T X)/2.
 // e = ||X^T X - I||_F / sqrt(n) is measured before every step (the Gram is the step's
 // own first half) and the steps stop once e reaches the rounding floor
-// max(1e-14, eps sqrt(m) / 2), once a step no longer halves e (rounding level), or
+// max(1e-14, eps sqrt(m) / 2), once a step no longer halves e (rounding level), after a
+// step whose bound on the next e is below a tenth of the floor (its Gram is not formed), or
 // after kNsMaxSteps.  Near convergence e -> 0.75 e^2; from e = 0.1 that is four steps.  On entry G holds the lower triangle of X^T X and e0 its
 // e.  Records the steps as branch 3 after the `it` Zolo iterations.
 void newton_schulz_finish(Context& c, int m, int n, double* X, int64_t ldx, Mat G, Mat Z, double e0, int it) {
@@ -241,6 +242,11 @@ void newton_schulz_finish(Context& c, int m, int n, double* X, int64_t ldx, Mat 
       c.stats.err[slot] = e;
     }
     c.stats.ns_steps++;
+    // with d_i = sigma_i^2 - 1 a step maps d to -3/4 d^2 (1 - d/3), so the next e is at most
+    // 3/4 e^2 sqrt(n) (1 + e sqrt(n)/3) plus the step's rounding: far below the floor, the next
+    // Gram would only confirm the floor and is not formed
+    const double rn = std::sqrt(static_cast<double>(n));
+    if (0.75 * e * e * rn * (1.0 + e * rn / 3.0) <= 0.1 * floor_e) break;
     // the next Gram: the measurement that decides whether another step is needed
     gemm(c, 1, 0, n, n, m, 1.0, Mat{X, ldx, 0}, Mat{X, ldx, 0}, 0.0, G, 1, nullptr, 1, 0);
     ck(ns_prepare(n, G.p, G.ld, c.dpartial(), scal + 2, 0, c.stream()));
